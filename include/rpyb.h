@@ -1,0 +1,226 @@
+/*
+ * rpyb.h -- C ABI of the B200 dense truncated tensor-algebra library
+ * (librpyb.so).  Plain C types only: device pointers are `void*`, sizes are
+ * int64_t, the CUDA stream is passed as an opaque `void*` (a cudaStream_t;
+ * NULL means the legacy default stream).
+ *
+ * Conventions shared by every entry point
+ * ---------------------------------------
+ *  - Return value: 0 on success, a negative RPYB_E* code on failure.  The
+ *    thread-local message of the last failure is rpyb_last_error().
+ *  - The caller owns every buffer.  Device pointers must be device memory
+ *    (or managed memory) of the current CUDA device.
+ *  - Tensor layout (identical to RoughPy's dense free tensors): degree-major,
+ *    level k of a width-d tensor starts at degree_begin[k] = (d^k - 1)/(d - 1);
+ *    inside a level, word (a_1 ... a_k) sits at sum_i a_i d^(k-i) (first letter
+ *    most significant).  A batch is `batch` rows, row b at base + b*ld.
+ *  - dtype: RPYB_F32 (float32 storage; products accumulated with compensated,
+ *    double-float two-sum/two-product arithmetic) or RPYB_F64.
+ *  - Degree bounds follow roughpy.compute: a max_degree of -1 (or larger than
+ *    depth) means `depth`.
+ *  - Calls are asynchronous with respect to the host unless stated.  They are
+ *    thread-safe and may run concurrently on different streams.
+ *  - Entry points that need temporary device memory take (workspace,
+ *    workspace_bytes).  Query the size with the matching *_workspace_size
+ *    function.  Passing workspace == NULL makes the library take stream-ordered
+ *    memory with cudaMallocAsync/cudaFreeAsync on `stream`.
+ */
+#ifndef RPYB_H
+#define RPYB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RPYB_API __attribute__((visibility("default")))
+#else
+#define RPYB_API
+#endif
+
+/* dtypes */
+#define RPYB_F32 0
+#define RPYB_F64 1
+
+/* status codes */
+#define RPYB_OK 0
+#define RPYB_E_INVALID (-1)   /* bad argument: shape, dtype, bounds, null pointer */
+#define RPYB_E_CUDA (-2)      /* a CUDA runtime call failed */
+#define RPYB_E_NOMEM (-3)     /* workspace too small / allocation failed */
+#define RPYB_E_TIMEOUT (-4)   /* a bounded device wait ran out */
+#define RPYB_E_UNSUPPORTED (-5)
+
+/* Thread-local message describing the most recent failure on this thread. */
+RPYB_API const char* rpyb_last_error(void);
+/* Library version string. */
+RPYB_API const char* rpyb_version(void);
+/* Number of scalars in a width/depth tensor: (width^(depth+1)-1)/(width-1). */
+RPYB_API int64_t rpyb_tensor_size(int32_t width, int32_t depth);
+
+/*
+ * out[b] += lhs[b] (x) rhs[b], truncated: the dense free-tensor fused
+ * multiply-add over a batch of rows.
+ * Replaces: roughpy_compute/dense/basic/free_tensor_fma.hpp:13-53
+ *           (rpy::compute::basic::ft_fma), reached from
+ *           roughpy/compute/_src/dense_basic.cpp:85-151 (py_dense_ft_fma).
+ * deg_bounds = {out_min, out_max, lhs_min, lhs_max, rhs_min, rhs_max}; NULL
+ * means {0,-1,0,-1,0,-1}.
+ */
+RPYB_API int rpyb_ft_fma(int dtype, int32_t width, int32_t depth, int64_t batch,
+                         void* out, const void* lhs, const void* rhs,
+                         int64_t ld_out, int64_t ld_lhs, int64_t ld_rhs,
+                         const int32_t* deg_bounds, void* stream);
+
+/*
+ * Row-gathered variant used by tree reductions: for i < n,
+ *   out[out_idx[i]] (+)= lhs[lhs_idx[i]] (x) rhs[rhs_idx[i]]
+ * with accumulate != 0 selecting += and 0 selecting =.  Index arrays are
+ * device int64 arrays; NULL means the identity.  Rows share one ld.
+ * No reference counterpart as one call: it batches
+ * roughpy_compute/dense/basic/free_tensor_fma.hpp:13-53 over index lists.
+ */
+RPYB_API int rpyb_ft_mul_gather(int dtype, int32_t width, int32_t depth, int64_t n,
+                                void* out, const void* lhs, const void* rhs,
+                                int64_t ld, const int64_t* out_idx,
+                                const int64_t* lhs_idx, const int64_t* rhs_idx,
+                                int accumulate, void* stream);
+
+/*
+ * lhs[b] <- lhs[b] (x) rhs[b] in place.
+ * Replaces: roughpy_compute/dense/basic/free_tensor_inplace_mul.hpp:13-87,
+ *           via roughpy/compute/_src/dense_basic.cpp:193-237.
+ * deg_bounds = {lhs_min, lhs_max, rhs_min, rhs_max}; NULL = full.
+ */
+RPYB_API int64_t rpyb_ft_inplace_mul_workspace_size(int dtype, int32_t width,
+                                                    int32_t depth, int64_t batch);
+RPYB_API int rpyb_ft_inplace_mul(int dtype, int32_t width, int32_t depth, int64_t batch,
+                                 void* lhs, const void* rhs, int64_t ld_lhs,
+                                 int64_t ld_rhs, const int32_t* deg_bounds,
+                                 void* workspace, size_t workspace_bytes,
+                                 void* stream);
+
+/*
+ * out[b] <- exp(arg[b]) (level 0 of arg ignored), Horner scheme.
+ * Replaces: roughpy_compute/dense/intermediate/free_tensor_exp.hpp:13-37 via
+ *           roughpy/compute/_src/dense_intermediate.cpp:62-96.
+ * out_depth: -1 = depth.  The reference uses the out bounds for arg too.
+ */
+RPYB_API int64_t rpyb_ft_exp_workspace_size(int dtype, int32_t width, int32_t depth,
+                                            int64_t batch);
+RPYB_API int rpyb_ft_exp(int dtype, int32_t width, int32_t depth, int64_t batch,
+                         void* out, const void* arg, int64_t ld_out, int64_t ld_arg,
+                         int32_t out_depth, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
+/*
+ * out[b] <- multiplier[b] * exp(exponent[b]) (level 0 of exponent ignored).
+ * Replaces: roughpy_compute/dense/intermediate/free_tensor_fmexp.hpp:15-40 via
+ *           roughpy/compute/_src/dense_intermediate.cpp:127-196.
+ */
+RPYB_API int64_t rpyb_ft_fmexp_workspace_size(int dtype, int32_t width,
+                                              int32_t depth, int64_t batch);
+RPYB_API int rpyb_ft_fmexp(int dtype, int32_t width, int32_t depth, int64_t batch,
+                           void* out, const void* multiplier, const void* exponent,
+                           int64_t ld_out, int64_t ld_mul, int64_t ld_exp,
+                           int32_t out_depth, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/*
+ * out[b] <- log(arg[b]), assuming arg level 0 == 1 (it is masked).  The
+ * series is always evaluated in float64 on the device (float32 rows are
+ * widened), because its alternating terms cancel.  As in the reference, the
+ * incoming out[b][0] is added to the first Horner coefficient (pass zeroed
+ * rows for the plain logarithm).
+ * Replaces: roughpy_compute/dense/intermediate/free_tensor_log.hpp:12-39 via
+ *           roughpy/compute/_src/dense_intermediate.cpp:204-294.
+ */
+RPYB_API int64_t rpyb_ft_log_workspace_size(int dtype, int32_t width, int32_t depth,
+                                            int64_t batch);
+RPYB_API int rpyb_ft_log(int dtype, int32_t width, int32_t depth, int64_t batch,
+                         void* out, const void* arg, int64_t ld_out, int64_t ld_arg,
+                         int32_t out_depth, int32_t arg_depth, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
+/*
+ * out[b] <- antipode(arg[b]): word reversal with sign (-1)^degree.
+ * Replaces: roughpy_compute/dense/basic/free_tensor_antipode.hpp:50-100 via
+ *           roughpy/compute/_src/dense_basic.cpp:244-330.
+ */
+RPYB_API int rpyb_ft_antipode(int dtype, int32_t width, int32_t depth, int64_t batch,
+                              void* out, const void* arg, int64_t ld_out,
+                              int64_t ld_arg, void* stream);
+
+/*
+ * out[b] += L*_{op[b]}(arg[b]): adjoint of left free-tensor multiplication
+ * (acts on shuffle tensors).  deg = {out_depth, op_depth, arg_depth} (-1 = depth).
+ * Replaces: roughpy_compute/dense/basic/free_tensor_adjoint_left_mul.hpp:11-77
+ *           via roughpy/compute/_src/dense_basic.cpp (py_dense_ft_adj_lmul).
+ */
+RPYB_API int rpyb_ft_adjoint_left_mul(int dtype, int32_t width, int32_t depth,
+                                      int64_t batch, void* out, const void* op,
+                                      const void* arg, int64_t ld_out, int64_t ld_op,
+                                      int64_t ld_arg, const int32_t* deg,
+                                      void* stream);
+
+/*
+ * Batched path signatures: for each stream s, with increments rows
+ * offsets[s] .. offsets[s+1]-1 of `increments` ([total, width] row-major),
+ *   out[s] = exp(x_0) (x) exp(x_1) (x) ... (x) exp(x_{L-1})   (Chen product)
+ * mode RPYB_F64: float64 increments/output, plain float64 arithmetic.
+ * mode RPYB_F32: float32 increments/output, float32 products with lazily
+ *   compensated (two-sum folded) accumulation of the running signature.
+ * One persistent launch; work items are taken longest-stream first from a
+ * device-side queue.  `order` (device int64[n_streams], nullable) gives the
+ * processing order (longest first is best); `offsets` is a device int64
+ * array of n_streams+1 entries.  An empty stream gives the unit tensor.
+ * Replaces: algebra/src/lite_context.h:542-563 (compute_signature: a chain of
+ *           fmexp over increments) and the reference recipe of chaining
+ *           roughpy_compute/dense/intermediate/free_tensor_fmexp.hpp:15-40.
+ */
+RPYB_API int64_t rpyb_signature_workspace_size(int mode, int32_t width, int32_t depth,
+                                               int64_t n_streams);
+RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                            const int64_t* offsets, const void* increments,
+                            void* out, int64_t ld_out, const int64_t* order,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Lie basis (Hall set) and the Lie <-> tensor maps, built on the host.
+ * rpyb_lie_basis_size: number of Hall keys of degree 1..depth (excludes the
+ * null key 0).  rpyb_lie_basis_data fills data[(size+1)*2] (parent pairs,
+ * row 0 = (0,0)) and degree_begin[depth+2], identical to
+ * roughpy/compute/_src/lie_basis.c:201-337 (construct_lie_basis).
+ */
+RPYB_API int64_t rpyb_lie_basis_size(int32_t width, int32_t depth);
+RPYB_API int rpyb_lie_basis_data(int32_t width, int32_t depth, int64_t* data,
+                                 int64_t* degree_begin);
+/*
+ * CSR form of the maps.  which = 0: l2t (tensor_size rows x lie_size cols),
+ * which = 1: t2l (lie_size rows x tensor_size cols, rbracketing / degree).
+ * Call with indices == NULL to get the number of stored entries (return
+ * value >= 0), then again with arrays of that size.  Values in float64.
+ * Replaces: roughpy/compute/_src/lie_basis.c:902-950 (l2t) and :1066-1200
+ *           (t2l), vendored/libalgebra_lite/include/libalgebra_lite/maps.h:131-210.
+ */
+RPYB_API int64_t rpyb_lie_map_csr(int32_t width, int32_t depth, int which,
+                                  int64_t* indptr, int64_t* indices, double* values);
+
+/*
+ * y[b] = scale * M x[b] for a CSR matrix M (device arrays, float64 values),
+ * batched over rows; x, y of dtype (float32 rows are computed in float64).
+ * Replaces: roughpy_compute/dense/basic/apply_sparse_linear_map.hpp:16-55 via
+ *           roughpy/compute/_src/dense_basic.cpp:564-620 and :1055-1150.
+ */
+RPYB_API int rpyb_sparse_map(int dtype, int64_t n_rows, int64_t n_cols, int64_t batch,
+                             const int64_t* indptr, const int64_t* indices,
+                             const double* values, void* y, const void* x,
+                             int64_t ld_y, int64_t ld_x, double scale, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RPYB_H */

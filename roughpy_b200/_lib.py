@@ -1,0 +1,110 @@
+"""ctypes binding of ``librpyb.so`` (the C ABI declared in ``include/rpyb.h``).
+
+The library is loaded from ``roughpy_b200/_lib/librpyb.so``; there is no
+fallback implementation.  Importing this module on a machine without the
+built library raises ``ImportError`` with the build command.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "_lib" / "librpyb.so"
+
+F32 = 0
+F64 = 1
+
+OK = 0
+E_INVALID = -1
+E_CUDA = -2
+E_NOMEM = -3
+E_TIMEOUT = -4
+E_UNSUPPORTED = -5
+
+if not LIB_PATH.exists():
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python -m roughpy_b200.build`")
+
+lib = ctypes.CDLL(str(LIB_PATH))
+
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+_dbl = ctypes.c_double
+_pi32 = ctypes.POINTER(ctypes.c_int32)
+_pi64 = ctypes.POINTER(ctypes.c_int64)
+_pdbl = ctypes.POINTER(ctypes.c_double)
+
+# name -> (restype, argtypes); kept in the order of include/rpyb.h
+SIGNATURES = {
+    "rpyb_last_error": (ctypes.c_char_p, []),
+    "rpyb_version": (ctypes.c_char_p, []),
+    "rpyb_tensor_size": (_i64, [_i32, _i32]),
+    "rpyb_ft_fma": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _pi32, _vp]),
+    "rpyb_ft_mul_gather": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,
+                                  _int, _vp]),
+    "rpyb_ft_inplace_mul_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
+    "rpyb_ft_inplace_mul": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _pi32, _vp, _sz,
+                                   _vp]),
+    "rpyb_ft_exp_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
+    "rpyb_ft_exp": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _i32, _vp, _sz, _vp]),
+    "rpyb_ft_fmexp_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
+    "rpyb_ft_fmexp": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp,
+                             _sz, _vp]),
+    "rpyb_ft_log_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
+    "rpyb_ft_log": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _i32, _i32, _vp, _sz,
+                           _vp]),
+    "rpyb_ft_antipode": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _vp]),
+    "rpyb_ft_adjoint_left_mul": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64,
+                                        _pi32, _vp]),
+    "rpyb_signature_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
+    "rpyb_signature": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "rpyb_lie_basis_size": (_i64, [_i32, _i32]),
+    "rpyb_lie_basis_data": (_int, [_i32, _i32, _pi64, _pi64]),
+    "rpyb_lie_map_csr": (_i64, [_i32, _i32, _int, _pi64, _pi64, _pdbl]),
+    "rpyb_sparse_map": (_int, [_int, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _dbl,
+                               _vp]),
+}
+
+for _name, (_res, _args) in SIGNATURES.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+class RPYBError(RuntimeError):
+    """A librpyb call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[rpyb {code}] {message}")
+        self.code = code
+
+
+def last_error() -> str:
+    msg = lib.rpyb_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int) -> None:
+    """Raise the Python exception matching a librpyb status code."""
+    if rc == OK:
+        return
+    msg = last_error()
+    if rc == E_INVALID:
+        raise ValueError(msg)
+    if rc == E_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    if rc == E_NOMEM:
+        raise MemoryError(msg)
+    raise RPYBError(rc, msg)
+
+
+def bounds(*vals) -> ctypes.Array:
+    return (ctypes.c_int32 * len(vals))(*[int(v) for v in vals])
+
+
+def version() -> str:
+    return lib.rpyb_version().decode()

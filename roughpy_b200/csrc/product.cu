@@ -1,0 +1,292 @@
+// Batched truncated free-tensor product kernel (sm_100a).
+//
+// Work decomposition.  Output level k (k >= 1) holds d^k words; write a word
+// as w = u * d^(k-1) + r with u its first letter.  For every split p >= 1 the
+// right factor R_{k-p}[w mod d^(k-p)] = R_{k-p}[r mod d^(k-p)] does not depend
+// on u, so one thread owns a suffix r and produces the d words
+// {u * d^(k-1) + r : u < d}: each right-factor word is loaded once and reused
+// d times from a register, each left-factor word L_p[u d^(p-1) + r / d^(k-p)]
+// is a warp broadcast for small p, and the top-level streams
+// (L_k, R_k, old out_k) are coalesced across consecutive r.  The (level, r)
+// pairs of all output levels are flattened into one index space that is cut
+// into tiles of TILE_R suffixes; blockIdx.x walks tiles of one row so that
+// a row's lower levels stay hot in L2, blockIdx.y walks rows.
+//
+// Arithmetic.  float64: the terms are added in the reference order (lhs
+// degree from high to low, free_tensor_fma.hpp:31-46) with FMA.  float32:
+// every term is formed with an exact two-product and accumulated in a
+// double-float (hi, lo) pair with two-sum, rounded once at the end.
+#include "product.cuh"
+
+#include <algorithm>
+
+namespace rpyb {
+namespace {
+
+constexpr int kThreads = 256;
+
+struct KArgs {
+    int width;
+    int klo, khi;
+    int64_t db[kMaxDepth + 2];
+    int64_t pw[kMaxDepth + 1];
+    int64_t fcum[kMaxDepth + 2];   // fcum[k] = sum_{j<k, j>=klo} d^(j-1)
+    int pmin[kMaxDepth + 1], pmax[kMaxDepth + 1];
+    double scale[kMaxDepth + 1];
+    int64_t ftotal;
+    int64_t tile_r;
+    bool accumulate, lhs0_from_mem;
+    double lhs0_add;
+    bool l0_write, l0_prod;
+    int l0_base;
+    double l0_const, scale0;
+    void* out;
+    const void* lhs;
+    const void* rhs;
+    const void* addend;
+    int64_t ld_out, ld_lhs, ld_rhs, ld_add;
+    const int64_t* out_idx;
+    const int64_t* lhs_idx;
+    const int64_t* rhs_idx;
+    int64_t batch;
+};
+
+template <typename T>
+struct Acc;
+
+template <>
+struct Acc<double> {
+    double v;
+    __device__ __forceinline__ void init(double x) { v = x; }
+    __device__ __forceinline__ void add(double a, double b) { v = fma(a, b, v); }
+    __device__ __forceinline__ double value() const { return v; }
+};
+
+template <>
+struct Acc<float> {
+    DF v;
+    __device__ __forceinline__ void init(float x) { v.hi = x; v.lo = 0.f; }
+    __device__ __forceinline__ void add(float a, float b) { df_add_prod(v, a, b); }
+    __device__ __forceinline__ float value() const { return df_value(v); }
+};
+
+template <int D>
+__device__ __forceinline__ int64_t divd(int64_t x, int d)
+{
+    if constexpr (D > 0) {
+        return x / D;
+    } else {
+        return x / d;
+    }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kThreads)
+product_kernel(const KArgs a)
+{
+    const int d = (D > 0) ? D : a.width;
+    const int64_t f_begin = (int64_t)blockIdx.x * a.tile_r;
+    const int64_t f_end = min(f_begin + a.tile_r, a.ftotal);
+
+    for (int64_t b = blockIdx.y; b < a.batch; b += gridDim.y) {
+        const int64_t ro = a.out_idx ? a.out_idx[b] : b;
+        const int64_t rl = a.lhs_idx ? a.lhs_idx[b] : b;
+        const int64_t rr = a.rhs_idx ? a.rhs_idx[b] : b;
+        T* __restrict__ out = static_cast<T*>(a.out) + ro * a.ld_out;
+        const T* __restrict__ lhs = static_cast<const T*>(a.lhs) + rl * a.ld_lhs;
+        const T* __restrict__ rhs = static_cast<const T*>(a.rhs) + rr * a.ld_rhs;
+        const T* __restrict__ add =
+            a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
+
+        const T lhs0 = (a.lhs0_from_mem ? __ldg(lhs) : T(0)) + T(a.lhs0_add);
+
+        if (a.l0_write && blockIdx.x == 0 && threadIdx.x == 0) {
+            T v0 = T(0);
+            if (a.l0_base == 1) v0 = out[0];
+            else if (a.l0_base == 2) v0 = add[0];
+            v0 += T(a.l0_const);
+            if (a.l0_prod) v0 += T(a.scale0) * (lhs0 * __ldg(rhs));
+            out[0] = v0;
+        }
+
+        for (int64_t f = f_begin + threadIdx.x; f < f_end; f += kThreads) {
+            int k = a.klo;
+            while (f >= a.fcum[k + 1]) ++k;
+            const int64_t r = f - a.fcum[k];
+            const int64_t dk1 = a.pw[k - 1];
+            const int64_t obase = a.db[k] + r;
+
+            Acc<T> acc[(D > 0) ? D : 16];
+#pragma unroll
+            for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
+                if (D > 0 || u < d) {
+                    acc[u].init(a.accumulate ? out[obase + u * dk1] : T(0));
+                }
+            }
+
+            const int pmax = a.pmax[k];
+            const int pmin = a.pmin[k];
+            if (pmax >= pmin) {
+                // suffix length s = k - p, starting at the largest lhs degree
+                int s = k - pmax;
+                int64_t q = r / a.pw[s];
+                int64_t m = r - q * a.pw[s];
+                for (int p = pmax; p >= pmin; --p) {
+                    if (p == 0) {
+                        const T* rk = rhs + a.db[k] + r;
+#pragma unroll
+                        for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
+                            if (D > 0 || u < d) acc[u].add(lhs0, __ldg(rk + u * dk1));
+                        }
+                    } else {
+                        const T rv = __ldg(rhs + a.db[s] + m);
+                        const T* lp = lhs + a.db[p] + q;
+                        const int64_t dp1 = a.pw[p - 1];
+#pragma unroll
+                        for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
+                            if (D > 0 || u < d) acc[u].add(__ldg(lp + u * dp1), rv);
+                        }
+                    }
+                    // advance to suffix length s + 1
+                    const int64_t q2 = divd<D>(q, d);
+                    m += (q - q2 * d) * a.pw[s];
+                    q = q2;
+                    ++s;
+                }
+            }
+
+            const T sc = T(a.scale[k]);
+#pragma unroll
+            for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
+                if (D > 0 || u < d) {
+                    const int64_t o = obase + u * dk1;
+                    T v;
+                    if (a.accumulate) {
+                        v = acc[u].value();
+                    } else {
+                        v = sc * acc[u].value();
+                        if (add) v += add[o];
+                    }
+                    out[o] = v;
+                }
+            }
+        }
+    }
+}
+
+template <typename TD, typename TS>
+__global__ void convert_rows_kernel(TD* dst, int64_t ld_dst, const TS* src, int64_t ld_src,
+                                    int64_t cols, int64_t batch)
+{
+    const int64_t total = cols * batch;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i / cols;
+        const int64_t c = i - b * cols;
+        dst[b * ld_dst + c] = static_cast<TD>(src[b * ld_src + c]);
+    }
+}
+
+template <typename T>
+int dispatch(const KArgs& a, dim3 grid, cudaStream_t stream)
+{
+    switch (a.width) {
+        case 2: product_kernel<T, 2><<<grid, kThreads, 0, stream>>>(a); break;
+        case 3: product_kernel<T, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 4: product_kernel<T, 4><<<grid, kThreads, 0, stream>>>(a); break;
+        case 5: product_kernel<T, 5><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6: product_kernel<T, 6><<<grid, kThreads, 0, stream>>>(a); break;
+        case 7: product_kernel<T, 7><<<grid, kThreads, 0, stream>>>(a); break;
+        case 8: product_kernel<T, 8><<<grid, kThreads, 0, stream>>>(a); break;
+        default:
+            if (a.width > 16) return fail(RPYB_E_UNSUPPORTED, "product kernel supports width <= 16");
+            product_kernel<T, 0><<<grid, kThreads, 0, stream>>>(a);
+            break;
+    }
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
+}  // namespace
+
+int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
+                   const ProductRows& rows, cudaStream_t stream)
+{
+    if (rows.batch <= 0) return RPYB_OK;
+    KArgs a{};
+    a.width = g.width;
+    a.klo = std::max(1, spec.klo);
+    a.khi = spec.khi;
+    for (int i = 0; i <= kMaxDepth + 1; ++i) a.db[i] = g.db[i];
+    for (int i = 0; i <= kMaxDepth; ++i) a.pw[i] = g.pw[i];
+    int64_t f = 0;
+    for (int k = 0; k <= kMaxDepth + 1; ++k) a.fcum[k] = 0;
+    for (int k = a.klo; k <= a.khi; ++k) {
+        a.fcum[k] = f;
+        f += g.pw[k - 1];
+    }
+    // sentinel entries above khi so the level search stops
+    for (int k = std::max(a.khi + 1, a.klo); k <= kMaxDepth + 1; ++k) a.fcum[k] = f;
+    a.ftotal = f;
+    for (int k = 0; k <= kMaxDepth; ++k) {
+        a.pmin[k] = spec.pmin[k];
+        a.pmax[k] = spec.pmax[k];
+        a.scale[k] = spec.scale[k];
+    }
+    a.accumulate = spec.accumulate;
+    a.lhs0_from_mem = spec.lhs0_from_mem;
+    a.lhs0_add = spec.lhs0_add;
+    a.l0_write = spec.l0_write;
+    a.l0_prod = spec.l0_prod;
+    a.l0_base = spec.l0_base;
+    a.l0_const = spec.l0_const;
+    a.scale0 = spec.scale0;
+    a.out = rows.out;
+    a.lhs = rows.lhs;
+    a.rhs = rows.rhs;
+    a.addend = rows.addend;
+    a.ld_out = rows.ld_out;
+    a.ld_lhs = rows.ld_lhs;
+    a.ld_rhs = rows.ld_rhs;
+    a.ld_add = rows.ld_add;
+    a.out_idx = rows.out_idx;
+    a.lhs_idx = rows.lhs_idx;
+    a.rhs_idx = rows.rhs_idx;
+    a.batch = rows.batch;
+
+    // Suffixes per tile: about 4096 output words per CTA (>= one per thread).
+    a.tile_r = std::max<int64_t>(kThreads, 4096 / std::max(1, g.width));
+    int64_t tiles = (a.ftotal + a.tile_r - 1) / a.tile_r;
+    if (tiles == 0) tiles = 1;  // level 0 only
+    if (tiles > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "tensor too large");
+    dim3 grid((unsigned)tiles, (unsigned)std::min<int64_t>(rows.batch, 65535), 1);
+    if (dtype == RPYB_F64) return dispatch<double>(a, grid, stream);
+    return dispatch<float>(a, grid, stream);
+}
+
+int launch_convert_rows(int dst_dtype, void* dst, int64_t ld_dst, int src_dtype,
+                        const void* src, int64_t ld_src, int64_t cols, int64_t batch,
+                        cudaStream_t stream)
+{
+    if (cols <= 0 || batch <= 0) return RPYB_OK;
+    const int64_t total = cols * batch;
+    const int threads = 256;
+    const int64_t blocks = std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
+    if (dst_dtype == RPYB_F64 && src_dtype == RPYB_F32) {
+        convert_rows_kernel<double, float><<<(unsigned)blocks, threads, 0, stream>>>(
+            static_cast<double*>(dst), ld_dst, static_cast<const float*>(src), ld_src, cols, batch);
+    } else if (dst_dtype == RPYB_F32 && src_dtype == RPYB_F64) {
+        convert_rows_kernel<float, double><<<(unsigned)blocks, threads, 0, stream>>>(
+            static_cast<float*>(dst), ld_dst, static_cast<const double*>(src), ld_src, cols, batch);
+    } else if (dst_dtype == RPYB_F64) {
+        convert_rows_kernel<double, double><<<(unsigned)blocks, threads, 0, stream>>>(
+            static_cast<double*>(dst), ld_dst, static_cast<const double*>(src), ld_src, cols, batch);
+    } else {
+        convert_rows_kernel<float, float><<<(unsigned)blocks, threads, 0, stream>>>(
+            static_cast<float*>(dst), ld_dst, static_cast<const float*>(src), ld_src, cols, batch);
+    }
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
+}  // namespace rpyb

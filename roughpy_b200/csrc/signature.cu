@@ -1,0 +1,516 @@
+// Batched path signatures on sm_100a: S = exp(x_0) (x) exp(x_1) (x) ... for
+// thousands of streams of uneven length in one persistent launch.
+//
+// Decomposition.  For a level-1 increment x the Chen step S <- S (x) exp(x)
+// updates word w = (a_1 .. a_k) from S restricted to the prefixes of w:
+//
+//   S'_k[w] = sum_{j=0..k} S_{k-j}[a_1..a_{k-j}] x[a_{k-j+1}] ... x[a_k] / j!
+//
+// so the words under a fixed prefix evolve independently of every other
+// subtree.  One lane owns a level-(N-2) word pi (its "path" is the prefix
+// chain pi_1, pi_1 pi_2, ..., pi), G of pi's children at level N-1 and the
+// G*D top words below them.  The lane keeps everything it needs in
+// registers and recomputes the few shared ancestors (levels <= N-2) itself,
+// so lanes never communicate: there is no __syncthreads and no shared
+// state.  A warp takes 32 consecutive lanes of one stream from a device-side
+// queue (longest streams first) and walks that stream's increments.
+//
+// Per step, level k is evaluated by the Horner chain
+//   acc_1 = S_1 + x/k,  acc_i = S_i + acc_{i-1} (x) x/(k-i+1),  S'_k = S_k + acc_{k-1} (x) x
+// restricted to the lane's words, processing levels from the top down so that
+// every chain reads pre-step values (free_tensor_inplace_mul.hpp:22-85 uses the
+// same top-down order).
+//
+// Precision modes.  float64: plain double state and FMAs.  float32
+// ("compensated"): the products are float32, each word keeps its running
+// value as hi + lo plus a float32 delta accumulator that receives the step's
+// increment with one FMA; every `fold` steps the delta is folded into
+// (hi, lo) with an exact two-sum.  Chains read hi + delta.  The lo words of
+// the top level live in shared memory (they are touched only when folding).
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace rpyb {
+namespace {
+
+constexpr int kSigWarps = 8;  // warps per block of the persistent kernel
+
+struct SigArgs {
+    const int64_t* offsets;
+    const void* inc;
+    void* out;
+    int64_t ld_out;
+    const int64_t* order;
+    int64_t n_streams;
+    int64_t items_per_stream;
+    int64_t total_items;
+    int* queue;   // device work counter (zeroed before launch)
+    int fold;     // fold interval of the compensated mode (steps)
+    int64_t db[kMaxDepth + 2];
+};
+
+template <int D, int E>
+struct IPow {
+    static constexpr int64_t value = D * IPow<D, E - 1>::value;
+};
+template <int D>
+struct IPow<D, 0> {
+    static constexpr int64_t value = 1;
+};
+
+template <typename T, int D>
+__device__ __forceinline__ void load_row(T (&x)[D], const T* __restrict__ p)
+{
+    if constexpr (sizeof(T) == 4 && (D % 4) == 0) {
+#pragma unroll
+        for (int i = 0; i < D / 4; ++i) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i);
+            x[4 * i + 0] = v.x;
+            x[4 * i + 1] = v.y;
+            x[4 * i + 2] = v.z;
+            x[4 * i + 3] = v.w;
+        }
+    } else if constexpr (sizeof(T) == 8 && (D % 2) == 0) {
+#pragma unroll
+        for (int i = 0; i < D / 2; ++i) {
+            const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+            x[2 * i + 0] = v.x;
+            x[2 * i + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < D; ++i) x[i] = __ldg(p + i);
+    }
+}
+
+// F64 = true: double state; false: float32 compensated state.
+template <bool F64, int D, int N, int G>
+__global__ void __launch_bounds__(kSigWarps * 32)
+signature_kernel(const SigArgs a)
+{
+    using T = typename std::conditional<F64, double, float>::type;
+    constexpr int P = N - 2;                 // path levels 1..N-2
+    constexpr int SUBS = D / G;              // lanes sharing one level-(N-2) word
+    constexpr int64_t W = IPow<D, (P > 0 ? P : 0)>::value * SUBS;  // lanes per stream
+    constexpr int TOPW = G * D;              // top words per lane
+    static_assert(D % G == 0, "G must divide D");
+
+    extern __shared__ float smem_lo[];       // [warp][TOPW][32] lo words (float mode)
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float* lo_top = smem_lo + (size_t)warp * TOPW * 32;
+
+    while (true) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.total_items) break;
+
+        const int64_t slot = item / a.items_per_stream;
+        const int64_t blk = item - slot * a.items_per_stream;
+        const int64_t s = a.order ? a.order[slot] : slot;
+        const int64_t beta_raw = blk * 32 + lane;
+        const bool active = beta_raw < W;
+        const int64_t beta = active ? beta_raw : (W - 1);
+        const int64_t pi = beta / SUBS;
+        const int sub = (int)(beta - pi * SUBS);
+
+        int c[P > 0 ? P : 1];
+        {
+            int64_t t = pi;
+#pragma unroll
+            for (int i = P - 1; i >= 0; --i) {
+                c[i] = (int)(t % D);
+                t /= D;
+            }
+        }
+
+        const int64_t start = a.offsets[s];
+        const int64_t len = a.offsets[s + 1] - start;
+        const T* __restrict__ xs = static_cast<const T*>(a.inc) + start * D;
+
+        // ---- state
+        T ph[P > 0 ? P : 1], mh[G], th[G][D];
+        T pd[P > 0 ? P : 1], md[G], td[G][D];   // float mode: delta accumulators
+        T pl[P > 0 ? P : 1], ml[G];             // float mode: lo words
+#pragma unroll
+        for (int i = 0; i < (P > 0 ? P : 1); ++i) ph[i] = pd[i] = pl[i] = T(0);
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            mh[g] = md[g] = ml[g] = T(0);
+#pragma unroll
+            for (int b = 0; b < D; ++b) th[g][b] = td[g][b] = T(0);
+        }
+        if constexpr (!F64) {
+#pragma unroll
+            for (int w = 0; w < TOPW; ++w) lo_top[w * 32 + lane] = 0.f;
+        }
+
+        int since_fold = 0;
+        for (int64_t t = 0; t < len; ++t) {
+            const T* row = xs + t * D;
+            T x[D];
+            load_row<T, D>(x, row);
+            T xa[G];
+            // gather the lane's letters from the (L1-resident) row
+            {
+                const T* ra = row + sub * G;
+#pragma unroll
+                for (int g = 0; g < G; ++g) xa[g] = __ldg(ra + g);
+            }
+            T xc[P > 0 ? P : 1];
+#pragma unroll
+            for (int i = 0; i < P; ++i) xc[i] = __ldg(row + c[i]);
+
+            // pre-step values
+            T vp[P > 0 ? P : 1], vm[G];
+#pragma unroll
+            for (int i = 0; i < P; ++i) vp[i] = F64 ? ph[i] : (ph[i] + pd[i]);
+#pragma unroll
+            for (int g = 0; g < G; ++g) vm[g] = F64 ? mh[g] : (mh[g] + md[g]);
+
+            // ---- level N (top): chain through the path, then the mid words
+            {
+                T acc = T(1);
+                if constexpr (P > 0) {
+                    acc = vp[0] + xc[0] * (T(1) / T(N));
+#pragma unroll
+                    for (int i = 2; i <= P; ++i)
+                        acc = vp[i - 1] + acc * (xc[i - 1] * (T(1) / T(N - i + 1)));
+                }
+                const T accx = acc * (T(1) / T(2));
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    const T am = vm[g] + accx * xa[g];
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        if constexpr (F64) th[g][b] = fma(am, x[b], th[g][b]);
+                        else td[g][b] = fmaf(am, x[b], td[g][b]);
+                    }
+                }
+            }
+            // ---- level N-1 (mid words)
+            {
+                T acc = T(1);
+                if constexpr (P > 0) {
+                    acc = vp[0] + xc[0] * (T(1) / T(N - 1));
+#pragma unroll
+                    for (int i = 2; i <= P; ++i)
+                        acc = vp[i - 1] + acc * (xc[i - 1] * (T(1) / T(N - i)));
+                }
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    if constexpr (F64) mh[g] = fma(acc, xa[g], mh[g]);
+                    else md[g] = fmaf(acc, xa[g], md[g]);
+                }
+            }
+            // ---- path levels k = P .. 1
+#pragma unroll
+            for (int k = P; k >= 1; --k) {
+                T upd;
+                if (k == 1) {
+                    upd = xc[0];
+                } else {
+                    T acc = vp[0] + xc[0] * (T(1) / T(k));
+#pragma unroll
+                    for (int i = 2; i <= k - 1; ++i)
+                        acc = vp[i - 1] + acc * (xc[i - 1] * (T(1) / T(k - i + 1)));
+                    upd = acc * xc[k - 1];
+                }
+                if constexpr (F64) ph[k - 1] += upd;
+                else pd[k - 1] += upd;
+            }
+
+            if constexpr (!F64) {
+                if (++since_fold >= a.fold) {
+                    since_fold = 0;
+#pragma unroll
+                    for (int i = 0; i < P; ++i) {
+                        float sh, e;
+                        two_sum(ph[i], pd[i], sh, e);
+                        ph[i] = sh;
+                        pl[i] = __fadd_rn(pl[i], e);
+                        pd[i] = 0.f;
+                    }
+#pragma unroll
+                    for (int g = 0; g < G; ++g) {
+                        float sh, e;
+                        two_sum(mh[g], md[g], sh, e);
+                        mh[g] = sh;
+                        ml[g] = __fadd_rn(ml[g], e);
+                        md[g] = 0.f;
+#pragma unroll
+                        for (int b = 0; b < D; ++b) {
+                            two_sum(th[g][b], td[g][b], sh, e);
+                            th[g][b] = sh;
+                            float* lp = lo_top + (g * D + b) * 32 + lane;
+                            *lp = __fadd_rn(*lp, e);
+                            td[g][b] = 0.f;
+                        }
+                    }
+                }
+            }
+        }
+
+        // ---- write the stream's words owned by this lane
+        if (active) {
+            T* __restrict__ o = static_cast<T*>(a.out) + s * a.ld_out;
+            if (beta == 0) o[0] = T(1);
+            // path words: owned by the lane whose remaining digits are zero
+            {
+                bool zero_below = (sub == 0);
+                int64_t prefix = pi;
+#pragma unroll
+                for (int k = P; k >= 1; --k) {
+                    if (zero_below) {
+                        T v;
+                        if constexpr (F64) v = ph[k - 1];
+                        else v = (ph[k - 1] + (pl[k - 1] + pd[k - 1]));
+                        o[a.db[k] + prefix] = v;
+                    }
+                    zero_below = zero_below && (c[k - 1] == 0);
+                    prefix /= D;
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int64_t mw = pi * D + sub * G + g;
+                T v;
+                if constexpr (F64) v = mh[g];
+                else v = mh[g] + (ml[g] + md[g]);
+                o[a.db[N - 1] + mw] = v;
+#pragma unroll
+                for (int b = 0; b < D; ++b) {
+                    T tv;
+                    if constexpr (F64) tv = th[g][b];
+                    else tv = th[g][b] + (lo_top[(g * D + b) * 32 + lane] + td[g][b]);
+                    o[a.db[N] + mw * D + b] = tv;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------
+// Generic fallback for shapes without a specialised instantiation: one warp
+// per stream, state as a float64 row in the workspace, levels updated from
+// the top down with a warp barrier between levels.
+struct GenericTables {
+    int64_t db[kMaxDepth + 2];
+    int64_t pw[kMaxDepth + 1];
+};
+
+__global__ void signature_generic_kernel(int mode, int d, int n, const int64_t* offsets,
+                                         const void* inc, void* out, int64_t ld_out,
+                                         int64_t n_streams, double* state, int64_t T,
+                                         const GenericTables tab)
+{
+    const int64_t* db = tab.db;
+    const int64_t* pw = tab.pw;
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = wid; s < n_streams; s += nw) {
+        double* S = state + s * T;
+        for (int64_t i = lane; i < T; i += 32) S[i] = (i == 0) ? 1.0 : 0.0;
+        __syncwarp();
+        const int64_t start = offsets[s], len = offsets[s + 1] - start;
+        for (int64_t t = 0; t < len; ++t) {
+            const int64_t rowoff = (start + t) * d;
+            for (int k = n; k >= 1; --k) {
+                for (int64_t w = lane; w < pw[k]; w += 32) {
+                    // Horner over the prefixes of w: acc_i = S_i[w_1..w_i] + acc_{i-1} x[w_i]/(k-i+1)
+                    double acc = 1.0;
+                    for (int i = 1; i <= k; ++i) {
+                        const int64_t pref = w / pw[k - i];
+                        const int letter = (int)(pref % d);
+                        const double xv = (mode == RPYB_F64)
+                                              ? static_cast<const double*>(inc)[rowoff + letter]
+                                              : (double)static_cast<const float*>(inc)[rowoff + letter];
+                        const double scaled = acc * xv / (double)(k - i + 1);
+                        if (i < k) acc = S[db[i] + pref] + scaled;
+                        else acc = scaled;
+                    }
+                    S[db[k] + w] += acc;
+                }
+                __syncwarp();
+            }
+        }
+        for (int64_t i = lane; i < T; i += 32) {
+            if (mode == RPYB_F64) static_cast<double*>(out)[s * ld_out + i] = S[i];
+            else static_cast<float*>(out)[s * ld_out + i] = (float)S[i];
+        }
+        __syncwarp();
+    }
+}
+
+using SigKernel = void (*)(SigArgs);
+
+struct SigVariant {
+    SigKernel fn;
+    int g;
+    int64_t lanes;  // W
+    int top_words;
+};
+
+template <bool F64, int D, int N, int G>
+SigVariant make_variant()
+{
+    constexpr int64_t W = IPow<D, N - 2>::value * (D / G);
+    return SigVariant{&signature_kernel<F64, D, N, G>, G, W, G * D};
+}
+
+template <bool F64, int D, int G>
+bool pick_depth(int n, SigVariant& v)
+{
+    switch (n) {
+        case 2: v = make_variant<F64, D, 2, G>(); return true;
+        case 3: v = make_variant<F64, D, 3, G>(); return true;
+        case 4: v = make_variant<F64, D, 4, G>(); return true;
+        case 5: v = make_variant<F64, D, 5, G>(); return true;
+        case 6: v = make_variant<F64, D, 6, G>(); return true;
+        case 7:
+            if constexpr (D <= 4) { v = make_variant<F64, D, 7, G>(); return true; }
+            return false;
+        case 8:
+            if constexpr (D <= 3) { v = make_variant<F64, D, 8, G>(); return true; }
+            return false;
+        default: return false;
+    }
+}
+
+template <bool F64>
+bool pick_variant(int d, int n, SigVariant& v)
+{
+    switch (d) {
+        case 2: return pick_depth<F64, 2, 2>(n, v);
+        case 3: return pick_depth<F64, 3, 3>(n, v);
+        case 4: return pick_depth<F64, 4, 4>(n, v);
+        case 5: return pick_depth<F64, 5, 5>(n, v);
+        case 6: return pick_depth<F64, 6, 3>(n, v);
+        case 7: return pick_depth<F64, 7, 7>(n, v);
+        case 8: return pick_depth<F64, 8, 4>(n, v);
+        default: return false;
+    }
+}
+
+int device_sm_count()
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return sms;
+}
+
+}  // namespace
+
+int signature_fold_interval()
+{
+    static int fold = [] {
+        const char* e = getenv("RPYB_SIG_FOLD");
+        int f = e ? atoi(e) : 16;
+        return f > 0 ? f : 16;
+    }();
+    return fold;
+}
+
+}  // namespace rpyb
+
+using namespace rpyb;
+
+extern "C" {
+
+RPYB_API int64_t rpyb_signature_workspace_size(int mode, int32_t width, int32_t depth,
+                                               int64_t n_streams)
+{
+    Geometry g;
+    if (make_geometry(width, depth, g)) return -1;
+    SigVariant v;
+    const bool special = depth >= 2 && ((mode == RPYB_F64) ? pick_variant<true>(width, depth, v)
+                                                           : pick_variant<false>(width, depth, v));
+    int64_t bytes = 256;  // queue counter
+    if (!special) bytes += n_streams * g.size() * 8;
+    return bytes;
+}
+
+RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                            const int64_t* offsets, const void* increments, void* out,
+                            int64_t ld_out, const int64_t* order, void* workspace,
+                            size_t workspace_bytes, void* stream)
+{
+    int rc;
+    if (mode != RPYB_F32 && mode != RPYB_F64)
+        return fail(RPYB_E_INVALID, "unsupported signature mode");
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    if (n_streams < 0) return fail(RPYB_E_INVALID, "negative number of streams");
+    if (n_streams == 0) return RPYB_OK;
+    if (!offsets || !out) return fail(RPYB_E_INVALID, "null pointer");
+    if (n_streams > 1 && ld_out < g.size()) return fail(RPYB_E_INVALID, "ld_out too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t need = rpyb_signature_workspace_size(mode, width, depth, n_streams);
+    Scratch scratch(workspace, workspace_bytes, s);
+    void* ws = nullptr;
+    if ((rc = scratch.get((size_t)need, &ws))) return rc;
+
+    SigVariant v{};
+    const bool special = depth >= 2 && ((mode == RPYB_F64) ? pick_variant<true>(width, depth, v)
+                                                           : pick_variant<false>(width, depth, v));
+    const int sms = device_sm_count();
+    if (special) {
+        if (increments == nullptr) return fail(RPYB_E_INVALID, "null increments");
+        const bool vec = (mode == RPYB_F32) ? (width % 4 == 0) : (width % 2 == 0);
+        if (vec && (reinterpret_cast<uintptr_t>(increments) & 15) != 0)
+            return fail(RPYB_E_INVALID, "increments must be 16-byte aligned");
+        SigArgs a{};
+        a.offsets = offsets;
+        a.inc = increments;
+        a.out = out;
+        a.ld_out = ld_out;
+        a.order = order;
+        a.n_streams = n_streams;
+        a.items_per_stream = (v.lanes + 31) / 32;
+        a.total_items = a.items_per_stream * n_streams;
+        if (a.total_items > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "too many work items");
+        a.queue = static_cast<int*>(ws);
+        a.fold = signature_fold_interval();
+        for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
+        const size_t smem = (mode == RPYB_F64) ? 0 : (size_t)kSigWarps * v.top_words * 32 * 4;
+        static std::mutex mu;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        }
+        int per_sm = 0;
+        RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, kSigWarps * 32,
+                                                                smem));
+        if (per_sm < 1) per_sm = 1;
+        int64_t blocks = (int64_t)per_sm * sms;
+        const int64_t warps_needed = a.total_items;
+        blocks = std::min<int64_t>(blocks, (warps_needed + kSigWarps - 1) / kSigWarps);
+        if (blocks < 1) blocks = 1;
+        RPYB_CUDA(cudaMemsetAsync(ws, 0, sizeof(int), s));
+        v.fn<<<(unsigned)blocks, kSigWarps * 32, smem, s>>>(a);
+        RPYB_CUDA(cudaGetLastError());
+        return RPYB_OK;
+    }
+    // generic path
+    double* state = reinterpret_cast<double*>(static_cast<char*>(ws) + 256);
+    GenericTables tab;
+    for (int k = 0; k < kMaxDepth + 2; ++k) tab.db[k] = g.db[k];
+    for (int k = 0; k <= kMaxDepth; ++k) tab.pw[k] = g.pw[k];
+    const int64_t warps = std::min<int64_t>(n_streams, (int64_t)sms * 16);
+    const int threads = 128;
+    const int64_t blocks = (warps * 32 + threads - 1) / threads;
+    signature_generic_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+        mode, width, depth, offsets, increments, out, ld_out, n_streams, state, g.size(), tab);
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
+}  // extern "C"

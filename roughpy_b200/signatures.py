@@ -1,0 +1,118 @@
+"""Batched path signatures on the GPU.
+
+``signature(increments, offsets, depth, mode)`` computes, for every stream
+``s`` with increment rows ``offsets[s]:offsets[s+1]``, the Chen product
+``exp(x_0) (x) exp(x_1) (x) ...`` in the dense truncated free tensor algebra:
+the quantity RoughPy's ``Context.compute_signature`` /
+``LiteContext::compute_signature`` (algebra/src/lite_context.h:542-563)
+returns for one stream, for thousands of uneven streams in one launch.
+
+Modes: ``"f64"`` (float64 throughout) and ``"f32c"`` (float32 storage and
+products with compensated accumulation of the running signature).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+
+MODES = {"f64": _lib.F64, "f32c": _lib.F32}
+
+
+def tensor_size(width: int, depth: int) -> int:
+    n = int(_lib.lib.rpyb_tensor_size(int(width), int(depth)))
+    if n < 0:
+        raise ValueError(_lib.last_error())
+    return n
+
+
+def offsets_from_lengths(lengths) -> np.ndarray:
+    lengths = np.asarray(lengths, dtype=np.int64)
+    off = np.zeros(lengths.shape[0] + 1, dtype=np.int64)
+    np.cumsum(lengths, out=off[1:])
+    return off
+
+
+def longest_first(offsets) -> np.ndarray:
+    """Processing order for the device work queue: streams by length, longest first."""
+    offsets = np.asarray(offsets, dtype=np.int64)
+    lengths = np.diff(offsets)
+    return np.argsort(-lengths, kind="stable").astype(np.int64)
+
+
+class SignaturePlan:
+    """Device-side metadata for one batch layout (offsets + processing order).
+
+    Reusable across calls with the same stream lengths; holds the workspace
+    (work-queue counter) so repeated calls allocate nothing.
+    """
+
+    def __init__(self, offsets, width: int, depth: int, mode: str = "f32c", device="cuda"):
+        if mode not in MODES:
+            raise ValueError(f"mode must be one of {sorted(MODES)}")
+        self.width = int(width)
+        self.depth = int(depth)
+        self.mode = mode
+        self.code = MODES[mode]
+        off = np.asarray(offsets, dtype=np.int64)
+        if off.ndim != 1 or off.shape[0] < 1 or np.any(np.diff(off) < 0) or off[0] != 0:
+            raise ValueError("offsets must be a non-decreasing int array starting at 0")
+        self.n_streams = int(off.shape[0] - 1)
+        self.total = int(off[-1])
+        self.offsets_host = off
+        self.device = torch.device(device)
+        self.offsets = torch.from_numpy(off).to(self.device)
+        self.order = torch.from_numpy(longest_first(off)).to(self.device)
+        self.size = tensor_size(self.width, self.depth)
+        ws = int(_lib.lib.rpyb_signature_workspace_size(self.code, self.width, self.depth,
+                                                        self.n_streams))
+        if ws < 0:
+            raise ValueError(_lib.last_error())
+        self.workspace = torch.empty(max(ws, 1), dtype=torch.uint8, device=self.device)
+        self.dtype = torch.float64 if self.code == _lib.F64 else torch.float32
+
+    def run(self, increments: torch.Tensor, out: torch.Tensor | None = None,
+            stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+        """Launch on device tensors (no host synchronisation)."""
+        if increments.dtype != self.dtype:
+            raise TypeError(f"increments must be {self.dtype} for mode {self.mode}")
+        if not increments.is_cuda or not increments.is_contiguous():
+            raise ValueError("increments must be a contiguous CUDA tensor")
+        if increments.numel() != self.total * self.width:
+            raise ValueError("increments do not match the offsets")
+        if out is None:
+            out = torch.empty((self.n_streams, self.size), dtype=self.dtype, device=self.device)
+        s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+        _lib.check(_lib.lib.rpyb_signature(
+            self.code, self.width, self.depth, self.n_streams, self.offsets.data_ptr(),
+            increments.data_ptr(), out.data_ptr(), out.stride(0) if out.dim() > 1 else self.size,
+            self.order.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(), s))
+        return out
+
+
+def signature(increments, offsets=None, depth: int = 2, mode: str = "f32c", width=None):
+    """Signatures of a batch of streams.
+
+    ``increments``: array ``[total, width]`` (NumPy or torch; a single stream
+    may be given as ``[L, width]`` with ``offsets=None``).  Returns a tensor
+    ``[n_streams, tensor_size]`` on the GPU (or NumPy for NumPy input).
+    """
+    is_numpy = isinstance(increments, np.ndarray)
+    dt = np.float64 if mode == "f64" else np.float32
+    if is_numpy:
+        inc = torch.from_numpy(np.ascontiguousarray(increments, dtype=dt)).cuda()
+    else:
+        inc = increments.to(dtype=torch.float64 if mode == "f64" else torch.float32).contiguous()
+        if not inc.is_cuda:
+            inc = inc.cuda()
+    if inc.dim() != 2:
+        raise ValueError("increments must be two-dimensional [rows, width]")
+    w = int(width or inc.shape[1])
+    if offsets is None:
+        offsets = np.array([0, inc.shape[0]], dtype=np.int64)
+    plan = SignaturePlan(offsets, w, depth, mode, device=inc.device)
+    out = plan.run(inc)
+    if is_numpy:
+        return out.cpu().numpy()
+    return out

@@ -1,0 +1,72 @@
+"""The C-ABI library loads on a CPU-only host and exports its declared API.
+
+No kernel is launched here: only argument validation and host-side
+functions (sizes, Hall basis, Lie maps) are exercised.
+"""
+import ctypes
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "rpyb.h").read_text()
+    return sorted(set(re.findall(r"RPYB_API\s+[\w\s\*]+?\b(rpyb_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from roughpy_b200 import _lib
+    names = declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(_lib.lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_version_and_sizes():
+    from roughpy_b200 import _lib
+    assert "sm_100a" in _lib.version()
+    assert _lib.lib.rpyb_tensor_size(4, 5) == 1365
+    assert _lib.lib.rpyb_tensor_size(8, 5) == 37449
+    assert _lib.lib.rpyb_tensor_size(2, 12) == 8191
+    assert _lib.lib.rpyb_tensor_size(8, 6) == 299593
+    assert _lib.lib.rpyb_tensor_size(0, 3) == -1
+
+
+@pytest.mark.parametrize("call", [
+    # bad dtype
+    lambda L: L.rpyb_ft_fma(7, 2, 2, 1, 1, 1, 1, 7, 7, 7, None, None),
+    # null pointers
+    lambda L: L.rpyb_ft_fma(1, 2, 2, 1, None, None, None, 7, 7, 7, None, None),
+    # min degree above max degree
+    lambda L: L.rpyb_ft_fma(1, 2, 2, 1, 8, 8, 8, 7, 7, 7,
+                            (ctypes.c_int32 * 6)(2, 1, 0, -1, 0, -1), None),
+    # row stride smaller than the tensor
+    lambda L: L.rpyb_ft_fma(1, 2, 2, 4, 8, 8, 8, 3, 7, 7, None, None),
+    # depth out of range
+    lambda L: L.rpyb_ft_exp(1, 2, 99, 1, 8, 8, 7, 7, -1, None, 0, None),
+    lambda L: L.rpyb_signature(5, 2, 2, 1, 8, 8, 8, 7, None, None, 0, None),
+])
+def test_invalid_arguments_are_rejected_before_any_launch(call):
+    from roughpy_b200 import _lib
+    rc = call(_lib.lib)
+    assert rc == _lib.E_INVALID
+    assert _lib.last_error()
+
+
+def test_zero_batch_is_a_no_op():
+    from roughpy_b200 import _lib
+    assert _lib.lib.rpyb_ft_fma(1, 2, 2, 0, None, None, None, 7, 7, 7, None, None) == 0
+    assert _lib.lib.rpyb_signature(1, 2, 2, 0, None, None, None, 7, None, None, 0, None) == 0
+
+
+def test_python_errors_match_reference_types():
+    from roughpy_b200 import _internals
+    with pytest.raises(ValueError):
+        _internals._basis_wd(None)
+    with pytest.raises(TypeError):
+        _internals._dtype_code(np.int32)
