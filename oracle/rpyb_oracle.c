@@ -226,10 +226,11 @@ void orc_signature(int width, int depth, int64_t len, const double* inc, double*
     Geom g;
     geom_init(&g, width, depth);
     const int64_t n = g.db[depth + 1];
-    double* x = (double*)calloc((size_t)n, sizeof(double));
-    double* tmp = (double*)malloc(sizeof(double) * (size_t)n);
     memset(out, 0, sizeof(double) * (size_t)n);
     out[0] = 1.0;
+    if (depth == 0) return;
+    double* x = (double*)calloc((size_t)n, sizeof(double));
+    double* tmp = (double*)malloc(sizeof(double) * (size_t)n);
     for (int64_t t = 0; t < len; ++t) {
         for (int a = 0; a < width; ++a) x[1 + a] = inc[t * width + a];
         orc_ft_fmexp(width, depth, tmp, out, x, -1);

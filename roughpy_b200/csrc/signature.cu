@@ -25,8 +25,9 @@
 // ("compensated"): the products are float32, each word keeps its running
 // value as hi + lo plus a float32 delta accumulator that receives the step's
 // increment with one FMA; every `fold` steps the delta is folded into
-// (hi, lo) with an exact two-sum.  Chains read hi + delta.  The lo words of
-// the top level live in shared memory (they are touched only when folding).
+// (hi, lo) with an exact two-sum.  Chains read hi + (lo + delta), so the
+// value they see is never biased by the unfolded part.  The lo words of the
+// top level live in shared memory (they are touched only when folding).
 #include <algorithm>
 #include <mutex>
 #include <vector>
@@ -37,6 +38,7 @@ namespace rpyb {
 namespace {
 
 constexpr int kSigWarps = 8;  // warps per block of the persistent kernel
+constexpr int kChunk = 32;    // increment rows staged per warp in shared memory
 
 struct SigArgs {
     const int64_t* offsets;
@@ -86,9 +88,52 @@ __device__ __forceinline__ void load_row(T (&x)[D], const T* __restrict__ p)
     }
 }
 
+template <typename T, int D>
+__device__ __forceinline__ void store_row(T* __restrict__ p, const T (&x)[D])
+{
+    if constexpr (sizeof(T) == 4 && (D % 4) == 0) {
+#pragma unroll
+        for (int i = 0; i < D / 4; ++i)
+            reinterpret_cast<float4*>(p)[i] = make_float4(x[4 * i], x[4 * i + 1], x[4 * i + 2],
+                                                          x[4 * i + 3]);
+    } else if constexpr (sizeof(T) == 8 && (D % 2) == 0) {
+#pragma unroll
+        for (int i = 0; i < D / 2; ++i)
+            reinterpret_cast<double2*>(p)[i] = make_double2(x[2 * i], x[2 * i + 1]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < D; ++i) p[i] = x[i];
+    }
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void load_row_smem(T (&x)[D], const T* __restrict__ p)
+{
+    if constexpr (sizeof(T) == 4 && (D % 4) == 0) {
+#pragma unroll
+        for (int i = 0; i < D / 4; ++i) {
+            const float4 v = reinterpret_cast<const float4*>(p)[i];
+            x[4 * i + 0] = v.x;
+            x[4 * i + 1] = v.y;
+            x[4 * i + 2] = v.z;
+            x[4 * i + 3] = v.w;
+        }
+    } else if constexpr (sizeof(T) == 8 && (D % 2) == 0) {
+#pragma unroll
+        for (int i = 0; i < D / 2; ++i) {
+            const double2 v = reinterpret_cast<const double2*>(p)[i];
+            x[2 * i + 0] = v.x;
+            x[2 * i + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < D; ++i) x[i] = p[i];
+    }
+}
+
 // F64 = true: double state; false: float32 compensated state.
 template <bool F64, int D, int N, int G>
-__global__ void __launch_bounds__(kSigWarps * 32)
+__global__ void __launch_bounds__(kSigWarps * 32, F64 ? 1 : 2)
 signature_kernel(const SigArgs a)
 {
     using T = typename std::conditional<F64, double, float>::type;
@@ -98,10 +143,15 @@ signature_kernel(const SigArgs a)
     constexpr int TOPW = G * D;              // top words per lane
     static_assert(D % G == 0, "G must divide D");
 
-    extern __shared__ float smem_lo[];       // [warp][TOPW][32] lo words (float mode)
+    // dynamic shared memory: [warp][TOPW][32] lo words (float mode only),
+    // then [warp][kChunk][D] staged increments
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float* lo_top = smem_lo + (size_t)warp * TOPW * 32;
+    float* lo_top = reinterpret_cast<float*>(smem_raw) + (size_t)warp * TOPW * 32;
+    const int nwarps = (int)(blockDim.x >> 5);
+    T* xbuf = reinterpret_cast<T*>(smem_raw + (F64 ? 0 : (size_t)nwarps * TOPW * 32 * 4)) +
+              (size_t)warp * kChunk * D;
 
     while (true) {
         int item = 0;
@@ -149,28 +199,36 @@ signature_kernel(const SigArgs a)
             for (int w = 0; w < TOPW; ++w) lo_top[w * 32 + lane] = 0.f;
         }
 
+        // Increments are staged through shared memory kChunk rows at a time:
+        // lane l fetches row t0 + kChunk + l with vector loads while the warp
+        // works through rows t0 .. t0 + kChunk - 1, so the global-memory
+        // latency is paid once per chunk instead of once per step.
+        T nx[D];
+        if (lane < len) load_row<T, D>(nx, xs + (int64_t)lane * D);
         int since_fold = 0;
-        for (int64_t t = 0; t < len; ++t) {
-            const T* row = xs + t * D;
+        for (int64_t t0 = 0; t0 < len; t0 += kChunk) {
+            __syncwarp();
+            if (t0 + lane < len) store_row<T, D>(xbuf + lane * D, nx);
+            __syncwarp();
+            if (t0 + kChunk + lane < len) load_row<T, D>(nx, xs + (t0 + kChunk + lane) * D);
+            const int nsteps = (int)min((int64_t)kChunk, len - t0);
+            for (int j = 0; j < nsteps; ++j) {
+            const T* row = xbuf + j * D;
             T x[D];
-            load_row<T, D>(x, row);
+            load_row_smem<T, D>(x, row);
             T xa[G];
-            // gather the lane's letters from the (L1-resident) row
-            {
-                const T* ra = row + sub * G;
 #pragma unroll
-                for (int g = 0; g < G; ++g) xa[g] = __ldg(ra + g);
-            }
+            for (int g = 0; g < G; ++g) xa[g] = row[sub * G + g];
             T xc[P > 0 ? P : 1];
 #pragma unroll
-            for (int i = 0; i < P; ++i) xc[i] = __ldg(row + c[i]);
+            for (int i = 0; i < P; ++i) xc[i] = row[c[i]];
 
             // pre-step values
             T vp[P > 0 ? P : 1], vm[G];
 #pragma unroll
-            for (int i = 0; i < P; ++i) vp[i] = F64 ? ph[i] : (ph[i] + pd[i]);
+            for (int i = 0; i < P; ++i) vp[i] = F64 ? ph[i] : (ph[i] + (pl[i] + pd[i]));
 #pragma unroll
-            for (int g = 0; g < G; ++g) vm[g] = F64 ? mh[g] : (mh[g] + md[g]);
+            for (int g = 0; g < G; ++g) vm[g] = F64 ? mh[g] : (mh[g] + (ml[g] + md[g]));
 
             // ---- level N (top): chain through the path, then the mid words
             {
@@ -252,6 +310,7 @@ signature_kernel(const SigArgs a)
                         }
                     }
                 }
+            }
             }
         }
 
@@ -408,6 +467,16 @@ int device_sm_count()
 
 }  // namespace
 
+int signature_warps_per_block()
+{
+    static int wpb = [] {
+        const char* e = getenv("RPYB_SIG_WPB");
+        int w = e ? atoi(e) : kSigWarps;
+        return (w >= 1 && w <= kSigWarps) ? w : kSigWarps;
+    }();
+    return wpb;
+}
+
 int signature_fold_interval()
 {
     static int fold = [] {
@@ -479,7 +548,10 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
         a.queue = static_cast<int*>(ws);
         a.fold = signature_fold_interval();
         for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
-        const size_t smem = (mode == RPYB_F64) ? 0 : (size_t)kSigWarps * v.top_words * 32 * 4;
+        const size_t esz = (mode == RPYB_F64) ? 8 : 4;
+        const int wpb = signature_warps_per_block();
+        const size_t smem = ((mode == RPYB_F64) ? 0 : (size_t)wpb * v.top_words * 32 * 4) +
+                            (size_t)wpb * kChunk * width * esz;
         static std::mutex mu;
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -487,15 +559,14 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
                                            (int)smem));
         }
         int per_sm = 0;
-        RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, kSigWarps * 32,
-                                                                smem));
+        RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, wpb * 32, smem));
         if (per_sm < 1) per_sm = 1;
         int64_t blocks = (int64_t)per_sm * sms;
         const int64_t warps_needed = a.total_items;
-        blocks = std::min<int64_t>(blocks, (warps_needed + kSigWarps - 1) / kSigWarps);
+        blocks = std::min<int64_t>(blocks, (warps_needed + wpb - 1) / wpb);
         if (blocks < 1) blocks = 1;
         RPYB_CUDA(cudaMemsetAsync(ws, 0, sizeof(int), s));
-        v.fn<<<(unsigned)blocks, kSigWarps * 32, smem, s>>>(a);
+        v.fn<<<(unsigned)blocks, wpb * 32, smem, s>>>(a);
         RPYB_CUDA(cudaGetLastError());
         return RPYB_OK;
     }

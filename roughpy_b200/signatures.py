@@ -90,6 +90,17 @@ class SignaturePlan:
             self.order.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(), s))
         return out
 
+    def run_host(self, inc_host: torch.Tensor, out_host: torch.Tensor, inc_dev: torch.Tensor,
+                 out_dev: torch.Tensor) -> torch.Tensor:
+        """End-to-end call from (pinned) host buffers on the current stream:
+        host->device copy of the increments, the signature launch, and the
+        device->host copy of the signatures.  Asynchronous; synchronise the
+        stream before reading ``out_host``."""
+        inc_dev.copy_(inc_host, non_blocking=True)
+        self.run(inc_dev, out_dev)
+        out_host.copy_(out_dev, non_blocking=True)
+        return out_host
+
 
 def signature(increments, offsets=None, depth: int = 2, mode: str = "f32c", width=None):
     """Signatures of a batch of streams.
