@@ -116,6 +116,24 @@ RPYB_API int rpyb_ft_exp(int dtype, int32_t width, int32_t depth, int64_t batch,
                          void* stream);
 
 /*
+ * rpyb_ft_exp without any device allocation, for callers that cannot call
+ * cudaMalloc (a host application that owns every device allocation through a
+ * fixed pool, a thread where an allocation would synchronise the device, a
+ * callback that forbids allocation).  No counterpart in the reference: it is
+ * rpyb_ft_exp with its scratch taken from a file-scope device array of
+ * rpyb_ft_exp_noalloc_max_bytes() bytes (8 MiB) that every GPU loading the
+ * library holds until exit.  Calls needing more (batch * tensor_size *
+ * element size) fail with RPYB_E_INVALID.  The first call on a device looks
+ * up the array's device address; make it before any stream capture.  All
+ * calls on a device share the array, so calls that overlap on the GPU race:
+ * order them on one stream or with events.
+ */
+RPYB_API int64_t rpyb_ft_exp_noalloc_max_bytes(void);
+RPYB_API int rpyb_ft_exp_noalloc(int dtype, int32_t width, int32_t depth, int64_t batch,
+                                 void* out, const void* arg, int64_t ld_out, int64_t ld_arg,
+                                 int32_t out_depth, void* stream);
+
+/*
  * out[b] <- multiplier[b] * exp(exponent[b]) (level 0 of exponent ignored).
  * Replaces: roughpy_compute/dense/intermediate/free_tensor_fmexp.hpp:15-40 via
  *           roughpy/compute/_src/dense_intermediate.cpp:127-196.

@@ -24,7 +24,7 @@ E_UNSUPPORTED = -5
 
 if not LIB_PATH.exists():
     raise ImportError(
-        f"{LIB_PATH} is missing: build it with `python -m roughpy_b200.build`")
+        f"{LIB_PATH} is missing: build it with `python roughpy_b200/build.py`")
 
 lib = ctypes.CDLL(str(LIB_PATH))
 
@@ -51,6 +51,8 @@ SIGNATURES = {
                                    _vp]),
     "rpyb_ft_exp_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
     "rpyb_ft_exp": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _i32, _vp, _sz, _vp]),
+    "rpyb_ft_exp_noalloc_max_bytes": (_i64, []),
+    "rpyb_ft_exp_noalloc": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _i32, _vp]),
     "rpyb_ft_fmexp_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
     "rpyb_ft_fmexp": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp,
                              _sz, _vp]),

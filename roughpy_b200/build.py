@@ -1,6 +1,6 @@
 """Build the sm_100a shared library ``librpyb.so`` in-tree.
 
-``python -m roughpy_b200.build`` compiles every source under ``csrc/`` with
+``python roughpy_b200/build.py`` compiles every source under ``csrc/`` with
 nvcc for ``sm_100a`` only and links ``roughpy_b200/_lib/librpyb.so``.  Object
 files go to ``_build/`` at the repository root and are rebuilt only when a
 source or header is newer.
