@@ -7,10 +7,12 @@ built library raises ``ImportError`` with the build command.
 from __future__ import annotations
 
 import ctypes
+import os
 import pathlib
 
 _HERE = pathlib.Path(__file__).resolve().parent
-LIB_PATH = _HERE / "_lib" / "librpyb.so"
+# RPYB_LIB_PATH selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = pathlib.Path(os.environ.get("RPYB_LIB_PATH", _HERE / "_lib" / "librpyb.so"))
 
 F32 = 0
 F64 = 1

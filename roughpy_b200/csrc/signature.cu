@@ -24,10 +24,12 @@
 // Precision modes.  float64: plain double state and FMAs.  float32
 // ("compensated"): the products are float32, each word keeps its running
 // value as hi + lo plus a float32 delta accumulator that receives the step's
-// increment with one FMA; every `fold` steps the delta is folded into
-// (hi, lo) with an exact two-sum.  Chains read hi + (lo + delta), so the
-// value they see is never biased by the unfolded part.  The lo words of the
-// top level live in shared memory (they are touched only when folding).
+// increment with one FMA (top-level words two at a time with packed f32x2
+// FMAs); every `fold` steps (default 24) the delta is folded into (hi, lo)
+// with an exact two-sum and (hi, lo) is renormalised so that hi is the
+// rounded value.  Chains read hi + delta.  The top level's lo words (and at
+// width 8 its hi words too) live in shared memory: they are touched only
+// when folding, which leaves the registers to the delta accumulators.
 #include <algorithm>
 #include <mutex>
 #include <vector>
@@ -39,6 +41,11 @@ namespace {
 
 constexpr int kSigWarps = 8;  // warps per block of the persistent kernel
 constexpr int kChunk = 32;    // increment rows staged per warp in shared memory
+
+// level-(N-1) words per lane of the float64 kernel at width 8
+#ifndef RPYB_SIG_F64_G8
+#define RPYB_SIG_F64_G8 8
+#endif
 
 struct SigArgs {
     const int64_t* offsets;
@@ -131,9 +138,57 @@ __device__ __forceinline__ void load_row_smem(T (&x)[D], const T* __restrict__ p
     }
 }
 
+template <typename T, int K>
+__device__ __forceinline__ void load_slice(T (&v)[K], const T* __restrict__ p)
+{
+    // vector loads when the slice is a whole number of 16-byte chunks and
+    // starts on a 16-byte boundary (true for the shapes that use them)
+    if constexpr ((K * sizeof(T)) % 16 == 0) {
+        if constexpr (sizeof(T) == 4) {
+#pragma unroll
+            for (int i = 0; i < K / 4; ++i) {
+                const float4 q = reinterpret_cast<const float4*>(p)[i];
+                v[4 * i] = q.x;
+                v[4 * i + 1] = q.y;
+                v[4 * i + 2] = q.z;
+                v[4 * i + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < K / 2; ++i) {
+                const double2 q = reinterpret_cast<const double2*>(p)[i];
+                v[2 * i] = q.x;
+                v[2 * i + 1] = q.y;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; ++i) v[i] = p[i];
+    }
+}
+
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+
+// (hi, lo, delta) -> (hi', lo', 0) with hi' + lo' = hi + lo + delta up to the
+// rounding of lo, and hi' the correctly rounded value of the sum.
+__device__ __forceinline__ void fold_word(float& hi, float& lo, float& delta)
+{
+    float s, e;
+    two_sum(hi, delta, s, e);
+    const float l = __fadd_rn(lo, e);
+    const float h = __fadd_rn(s, l);
+    lo = __fsub_rn(l, __fsub_rn(h, s));
+    hi = h;
+    delta = 0.f;
+}
+
 // F64 = true: double state; false: float32 compensated state.
-template <bool F64, int D, int N, int G>
-__global__ void __launch_bounds__(kSigWarps * 32, F64 ? 1 : 2)
+// HS (float mode): the hi words of the top level live in shared memory next to
+// their lo words, leaving only the per-step delta accumulators in registers;
+// this lets one lane own more top words (G = D) within the register file.
+template <bool F64, int D, int N, int G, bool HS>
+__global__ void __launch_bounds__(kSigWarps * 32, 1)
 signature_kernel(const SigArgs a)
 {
     using T = typename std::conditional<F64, double, float>::type;
@@ -142,15 +197,24 @@ signature_kernel(const SigArgs a)
     constexpr int64_t W = IPow<D, (P > 0 ? P : 0)>::value * SUBS;  // lanes per stream
     constexpr int TOPW = G * D;              // top words per lane
     static_assert(D % G == 0, "G must divide D");
+    // float mode with an even width: top words are updated in f32x2 pairs
+    constexpr bool PACK = !F64 && (D % 2 == 0);
 
-    // dynamic shared memory: [warp][TOPW][32] lo words (float mode only),
+    static_assert(!HS || (!F64 && PACK), "hi words in shared memory need the packed float mode");
+    // words of top-level state per warp kept in shared memory: lo (float mode),
+    // plus hi when HS
+    constexpr int TOP_SMEM = F64 ? 0 : (HS ? 2 : 1) * TOPW * 32;
+
+    // dynamic shared memory: [warp][TOP_SMEM] top-level lo (then hi) words,
     // then [warp][kChunk][D] staged increments
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float* lo_top = reinterpret_cast<float*>(smem_raw) + (size_t)warp * TOPW * 32;
+    float* lo_top = reinterpret_cast<float*>(smem_raw) + (size_t)warp * TOP_SMEM;
+    float2* lo_top2 = reinterpret_cast<float2*>(lo_top);          // packed [TOPW/2][32]
+    float2* hi_top2 = reinterpret_cast<float2*>(lo_top + TOPW * 32);  // HS only
     const int nwarps = (int)(blockDim.x >> 5);
-    T* xbuf = reinterpret_cast<T*>(smem_raw + (F64 ? 0 : (size_t)nwarps * TOPW * 32 * 4)) +
+    T* xbuf = reinterpret_cast<T*>(smem_raw + (size_t)nwarps * TOP_SMEM * 4) +
               (size_t)warp * kChunk * D;
 
     while (true) {
@@ -196,7 +260,7 @@ signature_kernel(const SigArgs a)
         }
         if constexpr (!F64) {
 #pragma unroll
-            for (int w = 0; w < TOPW; ++w) lo_top[w * 32 + lane] = 0.f;
+            for (int w = 0; w < TOP_SMEM / 32; ++w) lo_top[w * 32 + lane] = 0.f;
         }
 
         // Increments are staged through shared memory kChunk rows at a time:
@@ -216,19 +280,17 @@ signature_kernel(const SigArgs a)
             const T* row = xbuf + j * D;
             T x[D];
             load_row_smem<T, D>(x, row);
-            T xa[G];
-#pragma unroll
-            for (int g = 0; g < G; ++g) xa[g] = row[sub * G + g];
-            T xc[P > 0 ? P : 1];
+            T xa[G];                               // the lane's letters of level N-1
+            load_slice<T, G>(xa, row + sub * G);
+            T xc[P > 0 ? P : 1];                   // the lane's path letters
 #pragma unroll
             for (int i = 0; i < P; ++i) xc[i] = row[c[i]];
 
-            // pre-step values
-            T vp[P > 0 ? P : 1], vm[G];
+            // pre-step values of the path words (float: hi + delta, hi being
+            // kept as the rounded value of hi + lo)
+            T vp[P > 0 ? P : 1];
 #pragma unroll
-            for (int i = 0; i < P; ++i) vp[i] = F64 ? ph[i] : (ph[i] + (pl[i] + pd[i]));
-#pragma unroll
-            for (int g = 0; g < G; ++g) vm[g] = F64 ? mh[g] : (mh[g] + (ml[g] + md[g]));
+            for (int i = 0; i < P; ++i) vp[i] = F64 ? ph[i] : (ph[i] + pd[i]);
 
             // ---- level N (top): chain through the path, then the mid words
             {
@@ -237,16 +299,30 @@ signature_kernel(const SigArgs a)
                     acc = vp[0] + xc[0] * (T(1) / T(N));
 #pragma unroll
                     for (int i = 2; i <= P; ++i)
-                        acc = vp[i - 1] + acc * (xc[i - 1] * (T(1) / T(N - i + 1)));
+                        acc = fma_t(acc, xc[i - 1] * (T(1) / T(N - i + 1)), vp[i - 1]);
                 }
                 const T accx = acc * (T(1) / T(2));
 #pragma unroll
                 for (int g = 0; g < G; ++g) {
-                    const T am = vm[g] + accx * xa[g];
+                    // am = S_{N-1} + acc * x/2; in float mode the delta joins the
+                    // product before the (large) hi word
+                    const T am = F64 ? fma_t(accx, xa[g], mh[g]) : (mh[g] + fma_t(accx, xa[g], md[g]));
+                    if constexpr (PACK) {
+                        // packed f32x2 FMAs: two top words per instruction
+                        const float2 am2 = make_float2(am, am);
 #pragma unroll
-                    for (int b = 0; b < D; ++b) {
-                        if constexpr (F64) th[g][b] = fma(am, x[b], th[g][b]);
-                        else td[g][b] = fmaf(am, x[b], td[g][b]);
+                        for (int h = 0; h < D / 2; ++h) {
+                            const float2 r = __ffma2_rn(am2, make_float2(x[2 * h], x[2 * h + 1]),
+                                                        make_float2(td[g][2 * h], td[g][2 * h + 1]));
+                            td[g][2 * h] = r.x;
+                            td[g][2 * h + 1] = r.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < D; ++b) {
+                            if constexpr (F64) th[g][b] = fma_t(am, x[b], th[g][b]);
+                            else td[g][b] = fma_t(am, x[b], td[g][b]);
+                        }
                     }
                 }
             }
@@ -257,12 +333,12 @@ signature_kernel(const SigArgs a)
                     acc = vp[0] + xc[0] * (T(1) / T(N - 1));
 #pragma unroll
                     for (int i = 2; i <= P; ++i)
-                        acc = vp[i - 1] + acc * (xc[i - 1] * (T(1) / T(N - i)));
+                        acc = fma_t(acc, xc[i - 1] * (T(1) / T(N - i)), vp[i - 1]);
                 }
 #pragma unroll
                 for (int g = 0; g < G; ++g) {
-                    if constexpr (F64) mh[g] = fma(acc, xa[g], mh[g]);
-                    else md[g] = fmaf(acc, xa[g], md[g]);
+                    if constexpr (F64) mh[g] = fma_t(acc, xa[g], mh[g]);
+                    else md[g] = fma_t(acc, xa[g], md[g]);
                 }
             }
             // ---- path levels k = P .. 1
@@ -275,7 +351,7 @@ signature_kernel(const SigArgs a)
                     T acc = vp[0] + xc[0] * (T(1) / T(k));
 #pragma unroll
                     for (int i = 2; i <= k - 1; ++i)
-                        acc = vp[i - 1] + acc * (xc[i - 1] * (T(1) / T(k - i + 1)));
+                        acc = fma_t(acc, xc[i - 1] * (T(1) / T(k - i + 1)), vp[i - 1]);
                     upd = acc * xc[k - 1];
                 }
                 if constexpr (F64) ph[k - 1] += upd;
@@ -285,28 +361,46 @@ signature_kernel(const SigArgs a)
             if constexpr (!F64) {
                 if (++since_fold >= a.fold) {
                     since_fold = 0;
+                    // Fold the deltas into (hi, lo) with an exact two-sum, then
+                    // renormalise (hi, lo) so that hi is the rounded value: the
+                    // chains read hi + delta.
 #pragma unroll
-                    for (int i = 0; i < P; ++i) {
-                        float sh, e;
-                        two_sum(ph[i], pd[i], sh, e);
-                        ph[i] = sh;
-                        pl[i] = __fadd_rn(pl[i], e);
-                        pd[i] = 0.f;
-                    }
+                    for (int i = 0; i < P; ++i) fold_word(ph[i], pl[i], pd[i]);
 #pragma unroll
                     for (int g = 0; g < G; ++g) {
-                        float sh, e;
-                        two_sum(mh[g], md[g], sh, e);
-                        mh[g] = sh;
-                        ml[g] = __fadd_rn(ml[g], e);
-                        md[g] = 0.f;
+                        fold_word(mh[g], ml[g], md[g]);
+                        if constexpr (PACK) {
+                            // packed fast two-sum (|hi| >= |delta| except while a word is
+                            // still near zero, where the lost error is second order)
 #pragma unroll
-                        for (int b = 0; b < D; ++b) {
-                            two_sum(th[g][b], td[g][b], sh, e);
-                            th[g][b] = sh;
-                            float* lp = lo_top + (g * D + b) * 32 + lane;
-                            *lp = __fadd_rn(*lp, e);
-                            td[g][b] = 0.f;
+                            for (int h = 0; h < D / 2; ++h) {
+                                float2* hp = hi_top2 + (g * (D / 2) + h) * 32 + lane;
+                                const float2 hi = HS ? *hp : make_float2(th[g][2 * h], th[g][2 * h + 1]);
+                                const float2 dl = make_float2(td[g][2 * h], td[g][2 * h + 1]);
+                                const float2 sm = __fadd2_rn(hi, dl);
+                                const float2 z = __ffma2_rn(hi, make_float2(-1.f, -1.f), sm);
+                                const float2 er = __ffma2_rn(z, make_float2(-1.f, -1.f), dl);
+                                float2* lp = lo_top2 + (g * (D / 2) + h) * 32 + lane;
+                                *lp = __fadd2_rn(*lp, er);
+                                if constexpr (HS) {
+                                    *hp = sm;
+                                } else {
+                                    th[g][2 * h] = sm.x;
+                                    th[g][2 * h + 1] = sm.y;
+                                }
+                                td[g][2 * h] = 0.f;
+                                td[g][2 * h + 1] = 0.f;
+                            }
+                        } else {
+#pragma unroll
+                            for (int b = 0; b < D; ++b) {
+                                float sh, e;
+                                two_sum(th[g][b], td[g][b], sh, e);
+                                th[g][b] = sh;
+                                float* lp = lo_top + (g * D + b) * 32 + lane;
+                                *lp = __fadd_rn(*lp, e);
+                                td[g][b] = 0.f;
+                            }
                         }
                     }
                 }
@@ -345,7 +439,15 @@ signature_kernel(const SigArgs a)
                 for (int b = 0; b < D; ++b) {
                     T tv;
                     if constexpr (F64) tv = th[g][b];
-                    else tv = th[g][b] + (lo_top[(g * D + b) * 32 + lane] + td[g][b]);
+                    else if constexpr (PACK) {
+                        const float2 l2 = lo_top2[(g * (D / 2) + b / 2) * 32 + lane];
+                        float hv = th[g][b];
+                        if constexpr (HS) {
+                            const float2 h2 = hi_top2[(g * (D / 2) + b / 2) * 32 + lane];
+                            hv = (b & 1) ? h2.y : h2.x;
+                        }
+                        tv = hv + (((b & 1) ? l2.y : l2.x) + td[g][b]);
+                    } else tv = th[g][b] + (lo_top[(g * D + b) * 32 + lane] + td[g][b]);
                     o[a.db[N] + mw * D + b] = tv;
                 }
             }
@@ -411,47 +513,54 @@ using SigKernel = void (*)(SigArgs);
 struct SigVariant {
     SigKernel fn;
     int g;
-    int64_t lanes;  // W
-    int top_words;
+    int64_t lanes;          // W: lanes per stream
+    int top_words;          // G * D
+    int top_smem_floats;    // per warp, top-level words kept in shared memory
 };
 
-template <bool F64, int D, int N, int G>
+template <bool F64, int D, int N, int G, bool HS>
 SigVariant make_variant()
 {
     constexpr int64_t W = IPow<D, N - 2>::value * (D / G);
-    return SigVariant{&signature_kernel<F64, D, N, G>, G, W, G * D};
+    constexpr int smem = F64 ? 0 : (HS ? 2 : 1) * G * D * 32;
+    return SigVariant{&signature_kernel<F64, D, N, G, HS>, G, W, G * D, smem};
 }
 
-template <bool F64, int D, int G>
+template <bool F64, int D, int G, bool HS>
 bool pick_depth(int n, SigVariant& v)
 {
     switch (n) {
-        case 2: v = make_variant<F64, D, 2, G>(); return true;
-        case 3: v = make_variant<F64, D, 3, G>(); return true;
-        case 4: v = make_variant<F64, D, 4, G>(); return true;
-        case 5: v = make_variant<F64, D, 5, G>(); return true;
-        case 6: v = make_variant<F64, D, 6, G>(); return true;
+        case 2: v = make_variant<F64, D, 2, G, HS>(); return true;
+        case 3: v = make_variant<F64, D, 3, G, HS>(); return true;
+        case 4: v = make_variant<F64, D, 4, G, HS>(); return true;
+        case 5: v = make_variant<F64, D, 5, G, HS>(); return true;
+        case 6: v = make_variant<F64, D, 6, G, HS>(); return true;
         case 7:
-            if constexpr (D <= 4) { v = make_variant<F64, D, 7, G>(); return true; }
+            if constexpr (D <= 4) { v = make_variant<F64, D, 7, G, HS>(); return true; }
             return false;
         case 8:
-            if constexpr (D <= 3) { v = make_variant<F64, D, 8, G>(); return true; }
+            if constexpr (D <= 3) { v = make_variant<F64, D, 8, G, HS>(); return true; }
             return false;
         default: return false;
     }
 }
 
+// Lane shapes per width: G level-(N-1) words (and G*D top words) per lane.
+// float mode at width 8 keeps the top-level hi words in shared memory so that
+// a lane can own all 64 top words below one level-(N-2) word.
 template <bool F64>
 bool pick_variant(int d, int n, SigVariant& v)
 {
     switch (d) {
-        case 2: return pick_depth<F64, 2, 2>(n, v);
-        case 3: return pick_depth<F64, 3, 3>(n, v);
-        case 4: return pick_depth<F64, 4, 4>(n, v);
-        case 5: return pick_depth<F64, 5, 5>(n, v);
-        case 6: return pick_depth<F64, 6, 3>(n, v);
-        case 7: return pick_depth<F64, 7, 7>(n, v);
-        case 8: return pick_depth<F64, 8, 4>(n, v);
+        case 2: return pick_depth<F64, 2, 2, false>(n, v);
+        case 3: return pick_depth<F64, 3, 3, false>(n, v);
+        case 4: return pick_depth<F64, 4, 4, false>(n, v);
+        case 5: return pick_depth<F64, 5, 5, false>(n, v);
+        case 6: return pick_depth<F64, 6, 3, false>(n, v);
+        case 7: return pick_depth<F64, 7, 7, false>(n, v);
+        case 8:
+            if constexpr (F64) return pick_depth<F64, 8, RPYB_SIG_F64_G8, false>(n, v);
+            else return pick_depth<F64, 8, 8, true>(n, v);
         default: return false;
     }
 }
@@ -470,9 +579,10 @@ int device_sm_count()
 int signature_warps_per_block()
 {
     static int wpb = [] {
+        // 0 = choose by occupancy; RPYB_SIG_WPB forces a block size
         const char* e = getenv("RPYB_SIG_WPB");
-        int w = e ? atoi(e) : kSigWarps;
-        return (w >= 1 && w <= kSigWarps) ? w : kSigWarps;
+        int w = e ? atoi(e) : 0;
+        return (w >= 1 && w <= kSigWarps) ? w : 0;
     }();
     return wpb;
 }
@@ -481,8 +591,8 @@ int signature_fold_interval()
 {
     static int fold = [] {
         const char* e = getenv("RPYB_SIG_FOLD");
-        int f = e ? atoi(e) : 16;
-        return f > 0 ? f : 16;
+        int f = e ? atoi(e) : 24;
+        return f > 0 ? f : 24;
     }();
     return fold;
 }
@@ -549,18 +659,36 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
         a.fold = signature_fold_interval();
         for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
         const size_t esz = (mode == RPYB_F64) ? 8 : 4;
-        const int wpb = signature_warps_per_block();
-        const size_t smem = ((mode == RPYB_F64) ? 0 : (size_t)wpb * v.top_words * 32 * 4) +
-                            (size_t)wpb * kChunk * width * esz;
+        const size_t smem_warp = (size_t)v.top_smem_floats * 4 + (size_t)kChunk * width * esz;
+        // Warps are independent, so the block size only matters for occupancy:
+        // take the block size that fits the most warps per SM (registers and
+        // shared memory are both per-warp here), preferring larger blocks.
         static std::mutex mu;
         {
             std::lock_guard<std::mutex> lk(mu);
             RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
+                                           (int)(smem_warp * kSigWarps)));
         }
+        int wpb = signature_warps_per_block();
         int per_sm = 0;
-        RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, wpb * 32, smem));
+        if (wpb == 0) {
+            int best_warps = -1;
+            for (int w = kSigWarps; w >= 1; --w) {
+                int bps = 0;
+                RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, v.fn, w * 32,
+                                                                        smem_warp * w));
+                if (bps * w > best_warps) {
+                    best_warps = bps * w;
+                    wpb = w;
+                    per_sm = bps;
+                }
+            }
+        } else {
+            RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, wpb * 32,
+                                                                    smem_warp * wpb));
+        }
         if (per_sm < 1) per_sm = 1;
+        const size_t smem = smem_warp * wpb;
         int64_t blocks = (int64_t)per_sm * sms;
         const int64_t warps_needed = a.total_items;
         blocks = std::min<int64_t>(blocks, (warps_needed + wpb - 1) / wpb);
