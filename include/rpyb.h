@@ -89,6 +89,17 @@ RPYB_API int rpyb_ft_mul_gather(int dtype, int32_t width, int32_t depth, int64_t
                                 int accumulate, void* stream);
 
 /*
+ * Mixed-precision form of rpyb_ft_mul_gather: float64 output and left rows,
+ * float32 right rows, products accumulated in float64.  Used to multiply
+ * float32-stored dyadic nodes into float64 query accumulators.  No separate
+ * reference counterpart (the reference has no mixed-precision product).
+ */
+RPYB_API int rpyb_ft_mul_gather_mixed(int32_t width, int32_t depth, int64_t n, double* out,
+                                      const double* lhs, const float* rhs, int64_t ld,
+                                      const int64_t* out_idx, const int64_t* lhs_idx,
+                                      const int64_t* rhs_idx, int accumulate, void* stream);
+
+/*
  * lhs[b] <- lhs[b] (x) rhs[b] in place.
  * Replaces: roughpy_compute/dense/basic/free_tensor_inplace_mul.hpp:13-87,
  *           via roughpy/compute/_src/dense_basic.cpp:193-237.
@@ -236,6 +247,21 @@ RPYB_API int rpyb_sparse_map(int dtype, int64_t n_rows, int64_t n_cols, int64_t 
                              const int64_t* indptr, const int64_t* indices,
                              const double* values, void* y, const void* x,
                              int64_t ld_y, int64_t ld_x, double scale, void* stream);
+
+/*
+ * Dissection of the clopen interval [inf, sup) into maximal dyadic pieces at
+ * resolution `tol`, in order.  Piece i is [k[i] / 2^p[i], (k[i]+1) / 2^p[i]).
+ * Writes at most `cap` pieces and returns the number of pieces (which may
+ * exceed cap), or a negative status.  Opencl intervals are rejected, as the
+ * reference does not implement them either.
+ * Replaces: intervals/src/dyadic_interval.cpp:191-224 (to_dyadic_intervals).
+ */
+RPYB_API int64_t rpyb_dyadic_dissect(double inf, double sup, int32_t tol, int clopen,
+                                     int64_t* k, int32_t* p, int64_t cap);
+/* Batched form: query q's pieces are written to [offsets[q], offsets[q+1]). */
+RPYB_API int rpyb_dyadic_dissect_batch(int64_t n, const double* inf, const double* sup,
+                                       const int32_t* tol, int clopen, int64_t* k,
+                                       int32_t* p, int64_t cap, int64_t* offsets);
 
 #ifdef __cplusplus
 }

@@ -48,6 +48,8 @@ SIGNATURES = {
     "rpyb_ft_fma": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _pi32, _vp]),
     "rpyb_ft_mul_gather": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,
                                   _int, _vp]),
+    "rpyb_ft_mul_gather_mixed": (_int, [_i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _int,
+                                        _vp]),
     "rpyb_ft_inplace_mul_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
     "rpyb_ft_inplace_mul": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _i64, _pi32, _vp, _sz,
                                    _vp]),
@@ -71,6 +73,8 @@ SIGNATURES = {
     "rpyb_lie_map_csr": (_i64, [_i32, _i32, _int, _pi64, _pi64, _pdbl]),
     "rpyb_sparse_map": (_int, [_int, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _dbl,
                                _vp]),
+    "rpyb_dyadic_dissect": (_i64, [_dbl, _dbl, _i32, _int, _vp, _vp, _i64]),
+    "rpyb_dyadic_dissect_batch": (_int, [_i64, _vp, _vp, _vp, _int, _vp, _vp, _i64, _vp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -80,7 +80,10 @@ __device__ __forceinline__ int64_t divd(int64_t x, int d)
     }
 }
 
-template <typename T, int D>
+// T: output, left factor and accumulation type; TR: right factor type
+// (TR = float with T = double is the mixed mode: float32 right factors
+// accumulated into float64 rows).
+template <typename T, typename TR, int D>
 __global__ void __launch_bounds__(kThreads)
 product_kernel(const KArgs a)
 {
@@ -94,7 +97,7 @@ product_kernel(const KArgs a)
         const int64_t rr = a.rhs_idx ? a.rhs_idx[b] : b;
         T* __restrict__ out = static_cast<T*>(a.out) + ro * a.ld_out;
         const T* __restrict__ lhs = static_cast<const T*>(a.lhs) + rl * a.ld_lhs;
-        const T* __restrict__ rhs = static_cast<const T*>(a.rhs) + rr * a.ld_rhs;
+        const TR* __restrict__ rhs = static_cast<const TR*>(a.rhs) + rr * a.ld_rhs;
         const T* __restrict__ add =
             a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
 
@@ -105,7 +108,7 @@ product_kernel(const KArgs a)
             if (a.l0_base == 1) v0 = out[0];
             else if (a.l0_base == 2) v0 = add[0];
             v0 += T(a.l0_const);
-            if (a.l0_prod) v0 += T(a.scale0) * (lhs0 * __ldg(rhs));
+            if (a.l0_prod) v0 += T(a.scale0) * (lhs0 * T(__ldg(rhs)));
             out[0] = v0;
         }
 
@@ -133,13 +136,13 @@ product_kernel(const KArgs a)
                 int64_t m = r - q * a.pw[s];
                 for (int p = pmax; p >= pmin; --p) {
                     if (p == 0) {
-                        const T* rk = rhs + a.db[k] + r;
+                        const TR* rk = rhs + a.db[k] + r;
 #pragma unroll
                         for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
-                            if (D > 0 || u < d) acc[u].add(lhs0, __ldg(rk + u * dk1));
+                            if (D > 0 || u < d) acc[u].add(lhs0, T(__ldg(rk + u * dk1)));
                         }
                     } else {
-                        const T rv = __ldg(rhs + a.db[s] + m);
+                        const T rv = T(__ldg(rhs + a.db[s] + m));
                         const T* lp = lhs + a.db[p] + q;
                         const int64_t dp1 = a.pw[p - 1];
 #pragma unroll
@@ -187,20 +190,20 @@ __global__ void convert_rows_kernel(TD* dst, int64_t ld_dst, const TS* src, int6
     }
 }
 
-template <typename T>
+template <typename T, typename TR>
 int dispatch(const KArgs& a, dim3 grid, cudaStream_t stream)
 {
     switch (a.width) {
-        case 2: product_kernel<T, 2><<<grid, kThreads, 0, stream>>>(a); break;
-        case 3: product_kernel<T, 3><<<grid, kThreads, 0, stream>>>(a); break;
-        case 4: product_kernel<T, 4><<<grid, kThreads, 0, stream>>>(a); break;
-        case 5: product_kernel<T, 5><<<grid, kThreads, 0, stream>>>(a); break;
-        case 6: product_kernel<T, 6><<<grid, kThreads, 0, stream>>>(a); break;
-        case 7: product_kernel<T, 7><<<grid, kThreads, 0, stream>>>(a); break;
-        case 8: product_kernel<T, 8><<<grid, kThreads, 0, stream>>>(a); break;
+        case 2: product_kernel<T, TR, 2><<<grid, kThreads, 0, stream>>>(a); break;
+        case 3: product_kernel<T, TR, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 4: product_kernel<T, TR, 4><<<grid, kThreads, 0, stream>>>(a); break;
+        case 5: product_kernel<T, TR, 5><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6: product_kernel<T, TR, 6><<<grid, kThreads, 0, stream>>>(a); break;
+        case 7: product_kernel<T, TR, 7><<<grid, kThreads, 0, stream>>>(a); break;
+        case 8: product_kernel<T, TR, 8><<<grid, kThreads, 0, stream>>>(a); break;
         default:
             if (a.width > 16) return fail(RPYB_E_UNSUPPORTED, "product kernel supports width <= 16");
-            product_kernel<T, 0><<<grid, kThreads, 0, stream>>>(a);
+            product_kernel<T, TR, 0><<<grid, kThreads, 0, stream>>>(a);
             break;
     }
     RPYB_CUDA(cudaGetLastError());
@@ -260,8 +263,9 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
     if (tiles == 0) tiles = 1;  // level 0 only
     if (tiles > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "tensor too large");
     dim3 grid((unsigned)tiles, (unsigned)std::min<int64_t>(rows.batch, 65535), 1);
-    if (dtype == RPYB_F64) return dispatch<double>(a, grid, stream);
-    return dispatch<float>(a, grid, stream);
+    if (dtype == RPYB_F64) return dispatch<double, double>(a, grid, stream);
+    if (dtype == kMixedF64F32) return dispatch<double, float>(a, grid, stream);
+    return dispatch<float, float>(a, grid, stream);
 }
 
 int launch_convert_rows(int dst_dtype, void* dst, int64_t ld_dst, int src_dtype,

@@ -42,7 +42,9 @@ struct ProductRows {
     int64_t batch = 0;
 };
 
-// dtype RPYB_F64 (double) or RPYB_F32 (float, compensated accumulation).
+// dtype RPYB_F64 (double), RPYB_F32 (float, compensated accumulation) or
+// kMixedF64F32 (double output and left factor, float right factor).
+constexpr int kMixedF64F32 = 2;
 int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
                    const ProductRows& rows, cudaStream_t stream);
 

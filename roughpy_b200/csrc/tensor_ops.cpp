@@ -213,6 +213,42 @@ RPYB_API int rpyb_ft_mul_gather(int dtype, int32_t width, int32_t depth, int64_t
     return launch_product(dtype, g, sp, rows, static_cast<cudaStream_t>(stream));
 }
 
+RPYB_API int rpyb_ft_mul_gather_mixed(int32_t width, int32_t depth, int64_t n, double* out,
+                                      const double* lhs, const float* rhs, int64_t ld,
+                                      const int64_t* out_idx, const int64_t* lhs_idx,
+                                      const int64_t* rhs_idx, int accumulate, void* stream)
+{
+    int rc;
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    if (n < 0) return fail(RPYB_E_INVALID, "negative batch");
+    if (n == 0) return RPYB_OK;
+    if (!out || !lhs || !rhs) return fail(RPYB_E_INVALID, "null tensor pointer");
+    if (ld < g.size()) return fail(RPYB_E_INVALID, "row stride smaller than the tensor size");
+    ProductSpec sp;
+    sp.klo = 1;
+    sp.khi = depth;
+    for (int k = 1; k <= depth; ++k) {
+        sp.pmax[k] = k;
+        sp.pmin[k] = 0;
+        sp.scale[k] = 1.0;
+    }
+    sp.accumulate = accumulate != 0;
+    sp.l0_write = true;
+    sp.l0_base = accumulate ? 1 : 0;
+    sp.l0_prod = true;
+    ProductRows rows;
+    rows.out = out;
+    rows.lhs = lhs;
+    rows.rhs = rhs;
+    rows.ld_out = rows.ld_lhs = rows.ld_rhs = ld;
+    rows.out_idx = out_idx;
+    rows.lhs_idx = lhs_idx;
+    rows.rhs_idx = rhs_idx;
+    rows.batch = n;
+    return launch_product(kMixedF64F32, g, sp, rows, static_cast<cudaStream_t>(stream));
+}
+
 RPYB_API int64_t rpyb_ft_inplace_mul_workspace_size(int dtype, int32_t width, int32_t depth,
                                                     int64_t batch)
 {

@@ -17,4 +17,4 @@ def pytest_configure(config):
 def golden():
     import numpy as np
     d = ROOT / "tests" / "golden"
-    return {name: np.load(d / f"{name}.npz") for name in ("tensor_ops", "lie_maps", "signatures")}
+    return {name: np.load(d / f"{name}.npz") for name in ("tensor_ops", "lie_maps", "signatures", "streams")}

@@ -161,9 +161,62 @@ def gen_signatures():
     return out
 
 
+def ref_arith(width, depth):
+    """Stream restatement arithmetic backed by the reference roughpy.compute."""
+    from oracle.streams_ref import Arith
+    tb = rpc.TensorBasis(width, depth)
+    lb = rpc.LieBasis(width, depth)
+    l2t = rpc.lie_to_tensor(rpc.Lie(np.eye(lb.size()), lb), tb).data.T.copy()
+    t2l = rpc.tensor_to_lie(rpc.FreeTensor(np.eye(tb.size()), tb), lb).data.T.copy()
+    return Arith(width, depth, l2t, t2l,
+                 lambda x: rpc.ft_exp(ft(np.asarray(x, dtype=np.float64), tb)).data,
+                 lambda a, x: rpc.ft_fmexp(ft(np.asarray(a, dtype=np.float64), tb),
+                                           ft(np.asarray(x, dtype=np.float64), tb)).data,
+                 lambda x: rpc.ft_log(ft(np.asarray(x, dtype=np.float64), tb)).data)
+
+
+def gen_streams():
+    """Stream queries through the restated DyadicCachingLayer, reference arithmetic."""
+    from oracle.streams_ref import StreamRef
+    out = {}
+    rng = np.random.default_rng(3)
+    cases = [
+        ("a", 2, 3, 40, None, None),      # default indices (resolution 0)
+        ("b", 3, 3, 64, "grid", 6),       # events on a 2^-6 grid, explicit resolution
+        ("c", 2, 4, 30, "random", None),  # random times, heuristic resolution
+        ("d", 3, 2, 25, "random", 3),     # coarse resolution: several events per leaf
+    ]
+    for tag, w, d, n, kind, res in cases:
+        ar = ref_arith(w, d)
+        inc = rng.normal(0, 0.3, size=(n, w))
+        if kind is None:
+            idx = None
+        elif kind == "grid":
+            idx = np.arange(n) / 64.0
+        else:
+            idx = np.sort(rng.uniform(0.0, 2.0, size=n))
+        st = StreamRef(ar, inc, idx, res)
+        s0, s1 = st.support
+        qs = [(s0, s1), (s0 - 1.0, s0), (s0 + 0.3 * (s1 - s0), s0 + 0.3 * (s1 - s0)),
+              (s1 + 0.5, s1 + 1.0)]
+        for _ in range(14):
+            a, b = np.sort(rng.uniform(s0 - 0.2, s1 + 0.2, size=2))
+            qs.append((float(a), float(b)))
+        qs = np.array(qs)
+        out[f"{tag}_inc"] = inc
+        out[f"{tag}_idx"] = np.array([]) if idx is None else idx
+        out[f"{tag}_meta"] = np.array([w, d, -1 if res is None else res])
+        out[f"{tag}_queries"] = qs
+        out[f"{tag}_resolution"] = np.array([st.resolution])
+        out[f"{tag}_logsig"] = np.stack([st.log_signature(a, b) for a, b in qs])
+        out[f"{tag}_sig"] = np.stack([st.signature(a, b) for a, b in qs])
+    return out
+
+
 if __name__ == "__main__":
     np.savez_compressed(HERE / "tensor_ops.npz", **gen_tensor_ops())
     np.savez_compressed(HERE / "lie_maps.npz", **gen_lie())
     np.savez_compressed(HERE / "signatures.npz", **gen_signatures())
+    np.savez_compressed(HERE / "streams.npz", **gen_streams())
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)

@@ -1,0 +1,154 @@
+"""GPU stream queries (roughpy_b200.streams) against the reference's stream
+semantics: golden fixtures computed with the reference's own arithmetic through
+the restated DyadicCachingLayer, the restatement itself on random streams, and
+the reference test suite's known answers.
+
+Tolerances: signatures (float64 tree) <= 1e-12 per-level relative; log
+signatures are compared with an absolute floor of 1e-12 x the level scale,
+because exact-zero levels (e.g. a single event) make a relative error
+meaningless.  The float32-compensated tree is held to 1e-6."""
+import numpy as np
+import pytest
+
+from oracle import streams_ref as R
+from roughpy_b200.streams import LieIncrementStream, RealInterval
+from tests._util import level_rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def lie_close(got, want, tol):
+    scale = max(1.0, float(np.max(np.abs(want))))
+    assert float(np.max(np.abs(np.asarray(got) - want))) <= tol * scale
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c", "d"])
+def test_queries_match_reference_golden(golden, tag):
+    g = golden["streams"]
+    w, d, res = (int(v) for v in g[f"{tag}_meta"])
+    idx = g[f"{tag}_idx"]
+    st = LieIncrementStream.from_increments(g[f"{tag}_inc"], indices=None if idx.size == 0 else idx,
+                                            width=w, depth=d,
+                                            resolution=None if res < 0 else res)
+    assert st.resolution == int(g[f"{tag}_resolution"][0])
+    q = g[f"{tag}_queries"]
+    lie = st.log_signature_batch(q[:, 0], q[:, 1]).cpu().numpy()
+    sig = st.signature_batch(q[:, 0], q[:, 1]).cpu().numpy()
+    lie_close(lie, g[f"{tag}_logsig"], 1e-12)
+    assert level_rel_err(sig, g[f"{tag}_sig"], w, d) <= 1e-12
+    # single-query API agrees with the batch
+    for i in (0, 4, 7):
+        lie_close(st.log_signature(q[i, 0], q[i, 1]), g[f"{tag}_logsig"][i], 1e-12)
+
+
+def _arith(golden, w, d):
+    from tests.test_streams_host import arith
+    return arith(golden, w, d)
+
+
+@pytest.mark.parametrize("w,d,n,res", [(2, 4, 200, 7), (3, 3, 150, None), (4, 2, 300, 4),
+                                       (3, 3, 90, 9)])
+def test_random_streams_against_restatement(golden, w, d, n, res):
+    rng = np.random.default_rng(w * 100 + n)
+    inc = rng.normal(0, 0.2, size=(n, w))
+    idx = np.sort(rng.uniform(-0.5, 1.5, size=n))
+    ref = R.StreamRef(_arith(golden, w, d), inc, idx, res)
+    st = LieIncrementStream.from_increments(inc, indices=idx, width=w, depth=d, resolution=res)
+    assert st.resolution == ref.resolution
+    qs = np.sort(rng.uniform(-0.7, 1.7, size=(25, 2)), axis=1)
+    got = st.signature_batch(qs[:, 0], qs[:, 1]).cpu().numpy()
+    want = np.stack([ref.signature(a, b) for a, b in qs])
+    assert level_rel_err(got, want, w, d) <= 1e-12
+    # explicit coarse and fine query resolutions
+    for qres in (2, ref.resolution + 3):
+        got = st.log_signature_batch(qs[:8, 0], qs[:8, 1], resolution=qres).cpu().numpy()
+        want = np.stack([ref.log_signature(a, b, qres) for a, b in qs[:8]])
+        lie_close(got, want, 1e-11)
+
+
+def test_reference_known_answers():
+    # tests/streams/test_lie_increment_path.py:96-130
+    s = LieIncrementStream.from_increments(np.array([[3, 7, 0], [0, 0, 1]]), depth=2,
+                                           coeffs="DPReal")
+    np.testing.assert_array_equal(s.signature(depth=1), [1, 3, 7, 1])
+    s = LieIncrementStream.from_increments(np.array([[3, 7, 0, 4], [0, 0, 1, 5]]), width=2,
+                                           depth=2)
+    np.testing.assert_array_equal(s.signature(depth=1), [1, 3, 7])
+    # :356-382 alignment with default and explicit resolution
+    s = LieIncrementStream.from_increments(np.array([[0., 1., 2.], [3., 4., 5.]]), depth=2)
+    np.testing.assert_array_equal(s.log_signature(RealInterval(0.0, 0.1))[:3], [0., 1., 2.])
+    for i in range(1, 10):
+        assert not np.any(s.log_signature(RealInterval(0.1 * i, 0.1 * (i + 1))))
+    s = LieIncrementStream.from_increments(np.array([[0., 1., 2.], [3., 4., 5.]]), depth=2,
+                                           resolution=4)
+    np.testing.assert_array_equal(s.log_signature(RealInterval(0.0, 0.1), resolution=4)[:3],
+                                  [0., 1., 2.])
+    # :290-332 level one is the sum of the increments
+    rng = np.random.default_rng(12345)
+    arr = rng.integers(0, 5, size=(4, 3))
+    s = LieIncrementStream.from_increments(arr, width=3, depth=2)
+    np.testing.assert_array_almost_equal(s.signature(RealInterval(0.0, 5.0), resolution=2)[:4],
+                                         np.hstack([[1.0], arr.sum(axis=0)]), 13)
+    s = LieIncrementStream.from_increments(arr.T, width=4, depth=2)
+    np.testing.assert_array_almost_equal(s.signature(RealInterval(0.0, 5.0))[:5],
+                                         np.hstack([[1.0], arr.sum(axis=1)]), 13)
+    # :474-501 one increment: the signature is exp(increment)
+    inc = np.array([1., 9., -6.])
+    s = LieIncrementStream.from_increments(inc[None, :], indices=np.array([0.0]), width=3,
+                                           depth=3)
+    l2 = np.einsum("i,j->ij", inc, inc) / 2
+    l3 = np.einsum("ij,k->ijk", l2, inc) / 3
+    np.testing.assert_array_almost_equal(s.signature(RealInterval(0., 1.)),
+                                         np.hstack([[1.0], inc, l2.ravel(), l3.ravel()]))
+
+
+def test_tree_like_paths_have_the_pruned_signature():
+    # tests/streams/test_lie_increment_path.py:427-471
+    def sig(path, depth=2):
+        inc = np.diff(np.asarray(path, dtype=np.float64), axis=0)
+        if inc.shape[0] == 0:
+            inc = np.zeros((1, 2))
+        return LieIncrementStream.from_increments(inc, width=2, depth=depth).signature()
+    tree_like = [[0.0, 0], [1, 3], [0, 0], [1, 5], [2, 5], [1, 5], [0, 6], [1, 5], [0, 0]]
+    np.testing.assert_array_almost_equal(sig(tree_like), sig([[0., 0.], [0., 0.]]))
+    tree_like = [[0.0, 0], [1, 1], [3, 1], [2, 1], [1, 1], [2, 0]]
+    np.testing.assert_array_almost_equal(sig(tree_like), sig([[0., 0.], [1., 1.], [2., 0]]))
+
+
+def test_general_lie_increments_use_the_exponential_path(golden):
+    # rows with bracket coordinates: leaves are products of exp(l2t(lie))
+    rng = np.random.default_rng(4)
+    lies = rng.normal(0, 0.3, size=(12, 3))          # (2,2) Lie dimension 3
+    idx = np.arange(12) / 8.0
+    ref = R.StreamRef(_arith(golden, 2, 2), lies, idx, 2)
+    st = LieIncrementStream.from_increments(lies, indices=idx, width=2, depth=2, resolution=2)
+    qs = np.array([[0.0, 1.5], [0.1, 0.9], [0.25, 0.5]])
+    got = st.signature_batch(qs[:, 0], qs[:, 1]).cpu().numpy()
+    want = np.stack([ref.signature(a, b) for a, b in qs])
+    assert level_rel_err(got, want, 2, 2) <= 1e-12
+
+
+def test_dyadic_queries_float32_tree_within_1e6():
+    """The dyadic-query workload shape at reduced size: 2^12 events at t_i = i 2^-12,
+    width 6, depth 5, resolution 12, queries rounded to the resolution."""
+    n = 1 << 12
+    rng = np.random.default_rng(3)
+    inc = rng.normal(0, np.sqrt(1.0 / n), size=(n, 6))
+    idx = np.arange(n) / n
+    q = np.sort(np.floor(rng.uniform(0, 1, size=(300, 2)) * n) / n, axis=1)
+    s64 = LieIncrementStream.from_increments(inc, indices=idx, width=6, depth=5, resolution=12)
+    s32 = LieIncrementStream.from_increments(inc.astype(np.float32), indices=idx, width=6,
+                                             depth=5, resolution=12)
+    assert s32.mode == "f32c"
+    sig64 = s64.signature_batch(q[:, 0], q[:, 1]).cpu().numpy()
+    sig32 = s32.signature_batch(q[:, 0], q[:, 1]).cpu().numpy()
+    # full-interval signature equals the plain Chen product of all increments
+    import oracle
+    full = s64.signature(0.0, 1.0)
+    assert level_rel_err(full, oracle.signature(6, 5, inc), 6, 5) <= 1e-11
+    # f32 tree against the f64 tree, same (float32-rounded) increments
+    s64b = LieIncrementStream.from_increments(inc.astype(np.float32).astype(np.float64),
+                                              indices=idx, width=6, depth=5, resolution=12)
+    ref = s64b.signature_batch(q[:, 0], q[:, 1]).cpu().numpy()
+    assert level_rel_err(sig32, ref, 6, 5) <= 1e-6
+    assert sig64.shape == sig32.shape

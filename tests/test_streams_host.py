@@ -1,0 +1,113 @@
+"""Host side of the stream path: the dyadic dissection in librpyb.so and the
+CPU restatement of the stream query logic (oracle/streams_ref.py), checked
+against the reference's own known answers.  No GPU needed."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import streams_ref as R
+from roughpy_b200 import _lib
+
+# tests/intervals/test_dyadic_interval.py:217-289 (RealInterval(inf, sup), tol, expected)
+KNOWN = [
+    ((0.0, 1.0), 1, [(0, 0)]),
+    ((0.0, 1.0), 5, [(0, 0)]),
+    ((-1.0, 1.0), 1, [(-1, 0), (0, 0)]),
+    ((-1.0, 1.5), 1, [(-1, 0), (0, 0), (2, 1)]),
+    ((-1.0, 1.25), 1, [(-1, 0), (0, 0)]),
+    ((-1.0, 1.25), 2, [(-1, 0), (0, 0), (4, 2)]),
+    ((0.0, 1.63451), 1, [(0, 0), (2, 1)]),
+    ((0.0, 1.63451), 2, [(0, 0), (2, 1)]),
+    ((0.0, 1.63451), 3, [(0, 0), (2, 1), (12, 3)]),
+    ((0.0, 1.63451), 7, [(0, 0), (2, 1), (12, 3), (208, 7)]),
+]
+
+
+def lib_dissect(a, b, tol):
+    k = np.zeros(256, np.int64)
+    p = np.zeros(256, np.int32)
+    n = _lib.lib.rpyb_dyadic_dissect(a, b, tol, 1, k.ctypes.data, p.ctypes.data, 256)
+    assert n >= 0, _lib.last_error()
+    return [(int(k[i]), int(p[i])) for i in range(n)]
+
+
+@pytest.mark.parametrize("iv,tol,expected", KNOWN)
+def test_dissection_known_answers(iv, tol, expected):
+    assert lib_dissect(iv[0], iv[1], tol) == expected
+    assert R.to_dyadic_intervals(iv[0], iv[1], tol) == expected
+
+
+def test_dissection_library_matches_restatement_and_tiles_the_interval():
+    rng = np.random.default_rng(11)
+    for _ in range(3000):
+        a, b = np.sort(rng.uniform(-3, 3, size=2))
+        tol = int(rng.integers(0, 20))
+        pieces = lib_dissect(a, b, tol)
+        assert pieces == R.to_dyadic_intervals(a, b, tol)
+        # consecutive, and covering [floor(a 2^tol), floor(b 2^tol)) / 2^tol
+        lo = math.floor(math.ldexp(a, tol))
+        hi = math.floor(math.ldexp(b, tol))
+        pos = lo
+        for k, p in pieces:
+            assert p <= tol
+            assert k << (tol - p) == pos
+            pos = (k + 1) << (tol - p)
+        assert pos == hi or (not pieces and lo == hi)
+
+
+def test_batched_dissection_and_errors():
+    infs = np.array([0.0, -1.0, 0.5])
+    sups = np.array([1.63451, 1.25, 0.5])
+    tols = np.array([7, 2, 4], dtype=np.int32)
+    k = np.zeros(64, np.int64)
+    p = np.zeros(64, np.int32)
+    off = np.zeros(4, np.int64)
+    assert _lib.lib.rpyb_dyadic_dissect_batch(3, infs.ctypes.data, sups.ctypes.data,
+                                              tols.ctypes.data, 1, k.ctypes.data,
+                                              p.ctypes.data, 64, off.ctypes.data) == 0
+    assert list(off) == [0, 4, 7, 7]
+    assert _lib.lib.rpyb_dyadic_dissect(1.0, 0.0, 3, 1, None, None, 0) == _lib.E_INVALID
+    assert _lib.lib.rpyb_dyadic_dissect(0.0, 1.0, 3, 0, None, None, 0) == _lib.E_UNSUPPORTED
+
+
+def arith(golden, w, d):
+    g = golden["lie_maps"]
+    big = {(2, 2): (2, 4), (2, 3): (2, 4), (2, 4): (2, 4), (3, 2): (3, 3), (3, 3): (3, 3), (4, 2): (4, 3),
+           (4, 3): (4, 3)}[(w, d)]
+    l2t = g[f"w{big[0]}d{big[1]}_l2t_dense"]
+    t2l = g[f"w{big[0]}d{big[1]}_t2l_dense"]
+    T = (w ** (d + 1) - 1) // (w - 1)
+    L = int(np.count_nonzero(np.abs(l2t[:T]).sum(axis=0)))   # Lie keys of degree <= d
+    return R.Arith.from_oracle(w, d, l2t[:T, :L], t2l[:L, :T])
+
+
+def test_restated_stream_alignment_known_answers(golden):
+    # tests/streams/test_lie_increment_path.py:356-382
+    a = arith(golden, 3, 2)
+    st = R.StreamRef(a, np.array([[0., 1., 2.], [3., 4., 5.]]))
+    assert st.resolution == 0
+    np.testing.assert_array_equal(st.log_signature(0.0, 0.1)[:3], [0., 1., 2.])
+    for i in range(1, 10):
+        assert not np.any(st.log_signature(0.1 * i, 0.1 * (i + 1)))
+    st4 = R.StreamRef(a, np.array([[0., 1., 2.], [3., 4., 5.]]), resolution=4)
+    np.testing.assert_array_equal(st4.log_signature(0.0, 0.1, resolution=4)[:3], [0., 1., 2.])
+    for i in range(1, 10):
+        assert not np.any(st4.log_signature(0.1 * i, 0.1 * (i + 1), resolution=4))
+
+
+def test_restated_stream_level_one_sums_and_linear_signature(golden):
+    # tests/streams/test_lie_increment_path.py:290-332 and :474-501
+    rng = np.random.default_rng(12345)
+    arr = rng.integers(0, 5, size=(4, 3)).astype(np.float64)
+    a = arith(golden, 3, 2)
+    st = R.StreamRef(a, arr)
+    sig = st.signature(0.0, 5.0, 2)
+    np.testing.assert_array_almost_equal(sig[:4], np.hstack([[1.0], arr.sum(axis=0)]), 12)
+    a3 = arith(golden, 3, 3)
+    inc = np.array([1., 9., -6.])
+    st = R.StreamRef(a3, inc[None, :], indices=np.array([0.0]))
+    sig = st.signature(0.0, 1.0)
+    l2 = np.einsum("i,j->ij", inc, inc) / 2
+    l3 = np.einsum("ij,k->ijk", l2, inc) / 3
+    np.testing.assert_array_almost_equal(sig, np.hstack([[1.0], inc, l2.ravel(), l3.ravel()]))
