@@ -217,6 +217,28 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
                             void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Reverse-mode derivative of rpyb_signature: given the upstream gradient
+ * grad_sig (dLoss/dS per stream, [n_streams, T] with row stride ld_grad, or
+ * one shared row when ld_grad == 0), writes grad_inc = dLoss/d increments
+ * ([total, width]).  One block per stream walks it backwards: the states are
+ * checkpointed every `checkpoint_every` steps by a float64 forward pass and
+ * recomputed per segment; each step is differentiated through its Horner
+ * chains (reverse Chen products).  The gradient accumulator is float64 in
+ * both modes.  `max_len` must bound every stream length (it sizes the
+ * checkpoint scratch); longer streams get NaN gradients.  Width <= 8.
+ * No reference counterpart: RoughPy only has the forward-mode derivative
+ * (algebra/src/lite_context.h:577-636, LiteContext::sig_derivative_impl).
+ */
+RPYB_API int64_t rpyb_signature_backward_workspace_size(int mode, int32_t width, int32_t depth,
+                                                        int64_t n_streams, int64_t max_len,
+                                                        int32_t checkpoint_every);
+RPYB_API int rpyb_signature_backward(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                                     const int64_t* offsets, int64_t max_len,
+                                     const void* increments, const void* grad_sig,
+                                     int64_t ld_grad, void* grad_inc, int32_t checkpoint_every,
+                                     void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * Lie basis (Hall set) and the Lie <-> tensor maps, built on the host.
  * rpyb_lie_basis_size: number of Hall keys of degree 1..depth (excludes the
  * null key 0).  rpyb_lie_basis_data fills data[(size+1)*2] (parent pairs,

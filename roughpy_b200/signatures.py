@@ -60,6 +60,7 @@ class SignaturePlan:
             raise ValueError("offsets must be a non-decreasing int array starting at 0")
         self.n_streams = int(off.shape[0] - 1)
         self.total = int(off[-1])
+        self.max_len = int(np.diff(off).max()) if self.n_streams else 0
         self.offsets_host = off
         self.device = torch.device(device)
         self.offsets = torch.from_numpy(off).to(self.device)
@@ -127,3 +128,42 @@ def signature(increments, offsets=None, depth: int = 2, mode: str = "f32c", widt
     if is_numpy:
         return out.cpu().numpy()
     return out
+
+
+class _SignatureFunction(torch.autograd.Function):
+    """Batched signatures with the hand-written adjoint kernel as backward."""
+
+    @staticmethod
+    def forward(ctx, increments, plan, checkpoint_every):
+        out = plan.run(increments.contiguous())
+        ctx.save_for_backward(increments)
+        ctx.plan = plan
+        ctx.checkpoint_every = int(checkpoint_every)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (inc,) = ctx.saved_tensors
+        plan = ctx.plan
+        grad = grad_out.to(inc.dtype).contiguous()
+        grad_inc = torch.empty_like(inc)
+        ws_bytes = int(_lib.lib.rpyb_signature_backward_workspace_size(
+            plan.code, plan.width, plan.depth, plan.n_streams, plan.max_len,
+            ctx.checkpoint_every))
+        if ws_bytes < 0:
+            raise ValueError(_lib.last_error())
+        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=inc.device)
+        _lib.check(_lib.lib.rpyb_signature_backward(
+            plan.code, plan.width, plan.depth, plan.n_streams, plan.offsets.data_ptr(),
+            plan.max_len, inc.data_ptr(), grad.data_ptr(), grad.stride(0), grad_inc.data_ptr(),
+            ctx.checkpoint_every, ws.data_ptr(), ws.numel(),
+            torch.cuda.current_stream(inc.device).cuda_stream))
+        return grad_inc, None, None
+
+
+def signature_with_grad(increments: torch.Tensor, plan: SignaturePlan,
+                        checkpoint_every: int = 64) -> torch.Tensor:
+    """Differentiable batched signatures: forward by the signature kernel,
+    backward by the reverse Chen product kernel (states recomputed from
+    checkpoints every ``checkpoint_every`` steps)."""
+    return _SignatureFunction.apply(increments, plan, checkpoint_every)

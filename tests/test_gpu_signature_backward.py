@@ -1,0 +1,118 @@
+"""GPU signature adjoint (reverse Chen products with checkpoint recomputation)
+against float64 references: a differentiable float64 torch Chen product (exact
+gradients by autograd), central finite differences (h = 1e-6) of the float64
+signature kernel, and the float64 kernel's own gradient for the float32 mode.
+Tolerances: float64 <= 1e-10 relative to the gradient's max magnitude against
+autograd, <= 1e-6 against finite differences; float32 <= 1e-5."""
+import numpy as np
+import pytest
+import torch
+
+from roughpy_b200 import signatures as S
+
+pytestmark = pytest.mark.gpu
+
+
+def torch_signature(inc, width, depth):
+    """Dense float64 Chen product of exp(x_t) written with torch ops (autograd)."""
+    levels = [torch.ones(1, dtype=inc.dtype, device=inc.device)]
+    for k in range(1, depth + 1):
+        levels.append(torch.zeros(width ** k, dtype=inc.dtype, device=inc.device))
+    for t in range(inc.shape[0]):
+        x = inc[t]
+        ex = [torch.ones(1, dtype=inc.dtype, device=inc.device)]
+        for k in range(1, depth + 1):
+            ex.append(torch.outer(ex[-1], x).reshape(-1) / k)
+        new = []
+        for k in range(depth + 1):
+            acc = torch.zeros(width ** k, dtype=inc.dtype, device=inc.device)
+            for j in range(k + 1):
+                acc = acc + torch.outer(levels[k - j], ex[j]).reshape(-1)
+            new.append(acc)
+        levels = new
+    return torch.cat(levels)
+
+
+@pytest.mark.parametrize("w,d,lens,K", [(2, 3, [7, 1, 0, 12], 4), (3, 4, [20, 33], 64),
+                                        (4, 3, [9, 16], 1), (5, 2, [11], 3)])
+def test_f64_gradient_equals_autograd(w, d, lens, K):
+    rng = np.random.default_rng(w + 10 * d)
+    off = S.offsets_from_lengths(lens)
+    inc = torch.from_numpy(rng.normal(0, 0.4, size=(int(off[-1]), w))).cuda()
+    T = S.tensor_size(w, d)
+    W = torch.from_numpy(rng.normal(size=(len(lens), T))).cuda()
+    plan = S.SignaturePlan(off, w, d, "f64")
+    x = inc.clone().requires_grad_(True)
+    sig = S.signature_with_grad(x, plan, checkpoint_every=K)
+    (sig * W).sum().backward()
+    got = x.grad
+    xr = inc.clone().requires_grad_(True)
+    loss = 0
+    for s in range(len(lens)):
+        loss = loss + (torch_signature(xr[off[s]:off[s + 1]], w, d) * W[s]).sum()
+    loss.backward()
+    want = xr.grad
+    scale = float(want.abs().max()) if want.numel() else 1.0
+    assert float((got - want).abs().max()) <= 1e-10 * max(scale, 1.0)
+    ref_sig = torch.stack([torch_signature(inc[off[s]:off[s + 1]], w, d)
+                           for s in range(len(lens))])
+    assert float((sig.detach() - ref_sig).abs().max()) <= 1e-12 * float(ref_sig.abs().max())
+
+
+def test_config5_shape_finite_differences_and_f32():
+    """512 x 1024 increments, width 5, depth 6, loss <W, sig> with W ~ N(0,1):
+    the float64 adjoint against central differences on 64 sampled coordinates,
+    and the float32-compensated adjoint against the float64 one."""
+    n, L, w, d = 512, 1024, 5, 6
+    rng = np.random.default_rng(4)
+    inc64 = torch.from_numpy(rng.normal(0, np.sqrt(1.0 / L), size=(n * L, w))).cuda()
+    off = np.arange(n + 1, dtype=np.int64) * L
+    T = S.tensor_size(w, d)
+    W = torch.from_numpy(rng.normal(size=(T,))).cuda()
+    plan64 = S.SignaturePlan(off, w, d, "f64")
+    x = inc64.clone().requires_grad_(True)
+    sig = S.signature_with_grad(x, plan64)
+    (sig * W).sum().backward()
+    g64 = x.grad.clone()
+    # central differences on sampled coordinates (one stream's signature changes)
+    h = 1e-6
+    picks = rng.choice(n * L * w, size=64, replace=False)
+    for flat in picks:
+        r, c = divmod(int(flat), w)
+        s = r // L
+        sub_off = np.array([0, L], dtype=np.int64)
+        sub = S.SignaturePlan(sub_off, w, d, "f64")
+        xs = inc64[s * L:(s + 1) * L].clone()
+        xs[r - s * L, c] += h
+        lp = float((sub.run(xs) * W).sum())
+        xs[r - s * L, c] -= 2 * h
+        lm = float((sub.run(xs) * W).sum())
+        fd = (lp - lm) / (2 * h)
+        assert abs(float(g64[r, c]) - fd) <= 1e-6 * max(1.0, abs(fd)), (r, c, fd, float(g64[r, c]))
+    # float32 compensated mode against the float64 gradient on a 64-stream slice
+    m = 64
+    sl = slice(0, m * L)
+    plan32 = S.SignaturePlan(off[:m + 1], w, d, "f32c")
+    x32 = inc64[sl].float().clone().requires_grad_(True)
+    sig32 = S.signature_with_grad(x32, plan32)
+    (sig32.double() * W).sum().backward()
+    planb = S.SignaturePlan(off[:m + 1], w, d, "f64")
+    xb = inc64[sl].float().double().clone().requires_grad_(True)
+    (S.signature_with_grad(xb, planb) * W).sum().backward()
+    err = float((x32.grad.double() - xb.grad).abs().max()) / float(xb.grad.abs().max())
+    assert err <= 1e-5, err
+
+
+def test_shared_gradient_row_and_checkpoint_interval_invariance():
+    rng = np.random.default_rng(8)
+    w, d = 3, 3
+    off = S.offsets_from_lengths([40, 17, 64])
+    inc = torch.from_numpy(rng.normal(0, 0.3, size=(int(off[-1]), w))).cuda()
+    plan = S.SignaturePlan(off, w, d, "f64")
+    grads = []
+    for K in (1, 5, 64, 1000):
+        x = inc.clone().requires_grad_(True)
+        S.signature_with_grad(x, plan, checkpoint_every=K).sum().backward()
+        grads.append(x.grad)
+    for g in grads[1:]:
+        assert float((g - grads[0]).abs().max()) <= 1e-12 * float(grads[0].abs().max())
