@@ -42,6 +42,7 @@ LEN_LO, LEN_HI = 16, 4096
 FMA_PER_STEP = 42792          # Horner Chen step at (8,5): sum_k sum_{i<=k} 8^i
 SWEEP = [(2, 12), (4, 8), (6, 6), (8, 6)]
 SWEEP_BATCH = 1024
+E2E_CHUNKS = 8
 SM_COUNT_B200 = 148
 FP32_LANES_PER_SM = 128
 # dram bytes per launch of the float32 signature kernel on this workload,
@@ -211,24 +212,26 @@ def run_b200(args, rank, world, local_rank):
         plan.run(inc_d, out_d)
     ev1.record(stream)
     barrier()
-    clk = clocks.stop() if clocks else None
     ms_total = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = ms_total / args.steps
     value = world * N_STREAMS / (ms_step / 1e3)
 
-    # ---- end to end through the C ABI from pinned host buffers
+    # ---- end to end through the C ABI (rpyb_signature_host) from pinned host
+    # buffers: host->device copies, kernels and device->host copies, chunked
+    # so that the transfers overlap the computation
     inc_h = torch.from_numpy(inc).pin_memory()
     out_h = torch.empty((N_STREAMS, T), dtype=torch.float32).pin_memory()
     for _ in range(args.warmup):
-        plan.run_host(inc_h, out_h, inc_d, out_d)
+        plan.run_host_pipelined(inc_h, out_h, n_chunks=E2E_CHUNKS)
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        plan.run_host(inc_h, out_h, inc_d, out_d)
+        plan.run_host_pipelined(inc_h, out_h, n_chunks=E2E_CHUNKS)
     e1.record(stream)
     barrier()
+    clk = clocks.stop() if clocks else None
     e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
     e2e_value = world * N_STREAMS / (e2e_ms / 1e3)
 
@@ -300,7 +303,9 @@ def run_b200(args, rank, world, local_rank):
             "e2e": {"value": round(e2e_value, 1), "unit": "streams/s",
                     "h2d_bytes_per_step": int(inc.nbytes),
                     "d2h_bytes_per_step": int(N_STREAMS * T * 4),
-                    "ms_per_step": round(e2e_ms, 4)},
+                    "ms_per_step": round(e2e_ms, 4),
+                    "path": f"rpyb_signature_host, pinned host buffers, {E2E_CHUNKS} chunks "
+                            "with copies overlapping kernels"},
             "gpu_launches": args.steps,
             "clocks": clk,
             "peaks_source": pk_kind,
@@ -362,6 +367,178 @@ def fma_sweep(dev, hbm_gbs):
             del A, B, C
     torch.cuda.empty_cache()
     return res
+
+
+# ------------------------------------------------------------- other workloads
+def _events_time(torch, fn, reps, warm=2):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def plain_f64_signatures(dev):
+    """256 streams x 128 increments, width 4, depth 5, float64 (the reference's
+    CPU-runnable case), with the reference timed on one core beside it."""
+    import torch
+    from roughpy_b200 import signatures as S
+    import oracle
+    rng = np.random.default_rng(0)
+    n, L, w, d = 256, 128, 4, 5
+    inc = rng.normal(0, np.sqrt(1.0 / 128), size=(n * L, w))
+    off = np.arange(n + 1, dtype=np.int64) * L
+    plan = S.SignaturePlan(off, w, d, "f64", device=dev)
+    x = torch.from_numpy(inc).to(dev)
+    out = torch.empty((n, plan.size), dtype=torch.float64, device=dev)
+    ms = _events_time(torch, lambda: plan.run(x, out), 50)
+    got = out.cpu().numpy()
+    want = oracle.signatures(w, d, inc[:16 * L], off[:17])
+    err = float(np.max(np.abs(got[:16] - want)) / np.max(np.abs(want)))
+    ref = {}
+    rpc = oracle.ref_compute()
+    if rpc is not None:
+        t0 = time.perf_counter()
+        _cpu_worker(("reference", w, d, [inc[s * L:(s + 1) * L] for s in range(32)]))
+        dt = time.perf_counter() - t0
+        ref = {"value": round(32 / dt, 1), "unit": "streams/s", "cores": 1, "kind": "reference",
+               "sample": "32 of the 256 streams, chained roughpy.compute ft_fmexp"}
+    return {"workload": "256 streams x 128 increments, width 4, depth 5, float64",
+            "value": round(n / (ms / 1e3), 1), "unit": "streams/s", "ms": round(ms, 4),
+            "max_rel_err_vs_oracle": err, "cpu_reference_1_core": ref}
+
+
+def dyadic_queries(dev):
+    """Dyadic-cache stream queries: 2^16 events at t_i = i 2^-16, width 6,
+    depth 5, resolution 16, 100000 clopen queries with endpoints on the 2^-16
+    grid; log-signatures (Chen reduction over cached dyadic nodes, float64 log
+    and Hall projection).  The reference's uncached recursion is estimated
+    from its timed two-element CBH times the exact number it would perform."""
+    import torch
+    from roughpy_b200.streams import LieIncrementStream
+    n = 1 << 16
+    rng = np.random.default_rng(3)
+    inc = rng.normal(0, np.sqrt(1.0 / n), size=(n, 6))
+    idx = np.arange(n) / n
+    nq = 100000
+    q = np.sort(np.floor(rng.uniform(0, 1, size=(nq, 2)) * n) / n, axis=1)
+    res = {"workload": "2^16 events, width 6, depth 5, resolution 16, 100000 queries"}
+    lies = {}
+    for mode, data in (("f32c", inc.astype(np.float32)),
+                       ("f64", inc.astype(np.float32).astype(np.float64))):
+        st = LieIncrementStream.from_increments(data, indices=idx, width=6, depth=5,
+                                                resolution=16, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st._build_tree()
+        torch.cuda.synchronize()
+        tb = time.perf_counter() - t0
+        st.log_signature_batch(q[:1000, 0], q[:1000, 1])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lie = st.log_signature_batch(q[:, 0], q[:, 1])
+        torch.cuda.synchronize()
+        tq = time.perf_counter() - t0
+        lies[mode] = lie.cpu().numpy()
+        res[mode] = {"tree_build_ms": round(tb * 1e3, 2), "queries_s": round(tq, 4),
+                     "value": round(nq / tq, 1), "unit": "queries/s (wall clock, host "
+                                                         "dissection included)"}
+        del st
+        torch.cuda.empty_cache()
+    scale = np.maximum(np.abs(lies["f64"]).max(axis=1, keepdims=True), 1e-300)
+    res["f32c_max_rel_err_vs_f64"] = float((np.abs(lies["f32c"] - lies["f64"]) / scale).max())
+    res["cpu_reference_estimate"] = _dyadic_reference_estimate(q)
+    return res
+
+
+def _dyadic_reference_estimate(q):
+    import oracle
+    rpc = oracle.ref_compute()
+    if rpc is None:
+        return None
+    from roughpy_b200.streams import _dissect_batch
+    R = 16
+    tols = np.full(q.shape[0], 0, dtype=np.int32)
+    for i, (a, b) in enumerate(q):
+        L = b - a
+        tols[i] = R if L == 0 else max(R, (-min(0, np.frexp(L)[1] - 1)) + 2)
+    k, p, off = _dissect_batch(q[:, 0], q[:, 1], tols)
+    # a piece of power p < R recurses to 2^(R-p) cached leaves and performs
+    # 2^(R-p) - 1 two-element CBHs; each query adds one final CBH
+    cbh2 = int(np.sum(np.where(p < R, (np.int64(1) << np.maximum(R - p, 0)) - 1, 0)))
+    finals = int(np.sum(np.diff(off) > 1))
+    tb = rpc.TensorBasis(6, 5)
+    lb = rpc.LieBasis(6, 5)
+    rng = np.random.default_rng(0)
+    a = rng.normal(0, 1e-2, size=lb.size())
+    b = rng.normal(0, 1e-2, size=lb.size())
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ta = rpc.lie_to_tensor(rpc.Lie(a, lb), tb)
+        tbb = rpc.lie_to_tensor(rpc.Lie(b, lb), tb)
+        x = rpc.ft_fmexp(rpc.ft_exp(ta), tbb)
+        rpc.tensor_to_lie(rpc.ft_log(x), lb)
+    per = (time.perf_counter() - t0) / reps
+    est = (cbh2 + finals) * per
+    return {"value": round(q.shape[0] / est, 6), "unit": "queries/s (estimated)",
+            "cores": 1, "kind": "reference",
+            "model": f"{cbh2 + finals} two-element CBHs for the 100000 queries x "
+                     f"{per * 1e3:.3f} ms measured per reference CBH at (6,5)",
+            "estimated_seconds": round(est, 1)}
+
+
+def signature_backward(dev):
+    """512 streams x 1024 increments, width 5, depth 6, loss <W, sig>; forward
+    by the signature kernel, backward by the adjoint kernel (checkpoint 64)."""
+    import torch
+    from roughpy_b200 import signatures as S
+    n, L, w, d = 512, 1024, 5, 6
+    rng = np.random.default_rng(4)
+    inc = rng.normal(0, np.sqrt(1.0 / L), size=(n * L, w))
+    off = np.arange(n + 1, dtype=np.int64) * L
+    T = S.tensor_size(w, d)
+    W = torch.from_numpy(rng.normal(size=(T,))).to(dev)
+    res = {"workload": "512 x 1024 increments, width 5, depth 6, loss <W, sig>"}
+    grads = {}
+    for mode, dt in (("f32c", torch.float32), ("f64", torch.float64)):
+        plan = S.SignaturePlan(off, w, d, mode, device=dev)
+        x0 = torch.from_numpy(inc).to(dev, dt)
+
+        def step():
+            x = x0.clone().requires_grad_(True)
+            sig = S.signature_with_grad(x, plan)
+            (sig.double() * W).sum().backward()
+            return x.grad
+        ms = _events_time(torch, step, 3, warm=1)
+        grads[mode] = step().double()
+        res[mode] = {"ms_forward_backward": round(ms, 3),
+                     "value": round(n / (ms / 1e3), 1), "unit": "streams/s"}
+    g64 = grads["f64"]
+    res["f32c_grad_max_rel_err_vs_f64"] = float((grads["f32c"] - g64).abs().max() /
+                                                g64.abs().max())
+    return res
+
+
+def profile_slice(n):
+    """One f32c and one f64 signature launch on an n-stream slice of the bench
+    workload (the case captured by ncu)."""
+    import torch
+    from roughpy_b200 import signatures as S
+    lens, off, inc = make_workload(2, n)
+    x32 = torch.from_numpy(inc).cuda()
+    for mode, x in (("f32c", x32), ("f64", x32.double())):
+        plan = S.SignaturePlan(off, WIDTH, DEPTH, mode)
+        out = torch.empty((n, plan.size), dtype=plan.dtype, device="cuda")
+        plan.run(x, out)
+        torch.cuda.synchronize()
+    print("profile slice done", n)
 
 
 # ------------------------------------------------------------- reference arm
@@ -442,7 +619,14 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the plain-f64, dyadic-query and backward workloads")
+    ap.add_argument("--profile-slice", type=int, default=0,
+                    help="run one launch per mode on an N-stream slice and exit")
     args = ap.parse_args()
+    if args.profile_slice:
+        profile_slice(args.profile_slice)
+        return
     if args.warmup < 3 and args.impl == "b200":
         log("note: warmup raised to 3")
         args.warmup = 3
@@ -462,11 +646,20 @@ def main():
     if world > 1:
         import datetime
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
         res, workload = run_b200(args, rank, world, local_rank)
         if rank == 0:
+            if not args.no_extra:
+                dev = torch.device("cuda", local_rank)
+                for key, fn in (("plain_f64_signatures", plain_f64_signatures),
+                                ("dyadic_queries", dyadic_queries),
+                                ("signature_backward", signature_backward)):
+                    try:
+                        res[key] = fn(dev)
+                    except Exception as exc:  # keep the headline line
+                        res[key] = {"error": f"{type(exc).__name__}: {exc}"}
             if not args.no_cpu:
                 res["cpu_baseline"] = cpu_baseline_leg(workload)
             print(json.dumps(res), flush=True)

@@ -217,6 +217,26 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
                             void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * rpyb_signature from host memory, end to end: increments [total, width] and
+ * the output [n_streams, ld_out] are HOST buffers (pin them for overlap),
+ * offsets_host is a host int64 array.  The streams are processed in n_chunks
+ * contiguous groups of about equal total length; the host->device copy of
+ * chunk i+1 and the device->host copy of chunk i-1 overlap the kernel of
+ * chunk i (two internal copy streams, double-buffered device chunks in
+ * device_buffer, sized by rpyb_signature_host_device_bytes; NULL = stream-
+ * ordered allocation).  Completion is ordered on `stream`: synchronise it
+ * before reading out_host.
+ * Replaces: the same reference path as rpyb_signature, called with host data.
+ */
+RPYB_API int64_t rpyb_signature_host_device_bytes(int mode, int32_t width, int32_t depth,
+                                                  int64_t n_streams, const int64_t* offsets_host,
+                                                  int32_t n_chunks);
+RPYB_API int rpyb_signature_host(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                                 const int64_t* offsets_host, const void* inc_host,
+                                 void* out_host, int64_t ld_out, int32_t n_chunks,
+                                 void* device_buffer, size_t device_bytes, void* stream);
+
+/*
  * Reverse-mode derivative of rpyb_signature: given the upstream gradient
  * grad_sig (dLoss/dS per stream, [n_streams, T] with row stride ld_grad, or
  * one shared row when ld_grad == 0), writes grad_inc = dLoss/d increments

@@ -68,6 +68,9 @@ SIGNATURES = {
                                         _pi32, _vp]),
     "rpyb_signature_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
     "rpyb_signature": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "rpyb_signature_host_device_bytes": (_i64, [_int, _i32, _i32, _i64, _vp, _i32]),
+    "rpyb_signature_host": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i32, _vp, _sz,
+                                   _vp]),
     "rpyb_signature_backward_workspace_size": (_i64, [_int, _i32, _i32, _i64, _i64, _i32]),
     "rpyb_signature_backward": (_int, [_int, _i32, _i32, _i64, _vp, _i64, _vp, _vp, _i64, _vp,
                                        _i32, _vp, _sz, _vp]),

@@ -91,6 +91,33 @@ class SignaturePlan:
             self.order.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(), s))
         return out
 
+    def run_host_pipelined(self, inc_host: torch.Tensor, out_host: torch.Tensor,
+                           n_chunks: int = 8) -> torch.Tensor:
+        """End-to-end call on host buffers through ``rpyb_signature_host``:
+        chunked, with the copies in both directions overlapping the kernels.
+        Pass pinned tensors; synchronise the current stream before reading."""
+        if inc_host.is_cuda or out_host.is_cuda:
+            raise ValueError("run_host_pipelined takes host tensors")
+        if inc_host.dtype != self.dtype or out_host.dtype != self.dtype:
+            raise TypeError(f"host buffers must be {self.dtype}")
+        if not inc_host.is_contiguous() or inc_host.numel() != self.total * self.width:
+            raise ValueError("increments do not match the offsets")
+        key = int(n_chunks)
+        if getattr(self, "_host_key", None) != key:
+            nbytes = int(_lib.lib.rpyb_signature_host_device_bytes(
+                self.code, self.width, self.depth, self.n_streams,
+                self.offsets_host.ctypes.data, key))
+            if nbytes < 0:
+                raise ValueError(_lib.last_error())
+            self._host_buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
+            self._host_key = key
+        _lib.check(_lib.lib.rpyb_signature_host(
+            self.code, self.width, self.depth, self.n_streams, self.offsets_host.ctypes.data,
+            inc_host.data_ptr(), out_host.data_ptr(), out_host.stride(0), key,
+            self._host_buf.data_ptr(), self._host_buf.numel(),
+            torch.cuda.current_stream(self.device).cuda_stream))
+        return out_host
+
     def run_host(self, inc_host: torch.Tensor, out_host: torch.Tensor, inc_dev: torch.Tensor,
                  out_dev: torch.Tensor) -> torch.Tensor:
         """End-to-end call from (pinned) host buffers on the current stream:

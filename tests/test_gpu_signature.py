@@ -76,3 +76,20 @@ def test_plan_reuse_and_torch_inputs():
     torch.cuda.synchronize()
     assert torch.equal(a, b)
     assert float(a[3, 0]) == 1.0 and float(a[3, 1:].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("mode,chunks", [("f32c", 1), ("f32c", 5), ("f64", 3)])
+def test_host_pipelined_entry_matches_device_path(mode, chunks):
+    rng = np.random.default_rng(13)
+    w, d = 8, 5
+    lens = rng.integers(0, 300, size=37)
+    off = S.offsets_from_lengths(lens)
+    dt = np.float64 if mode == "f64" else np.float32
+    inc = rng.normal(0, 0.05, size=(int(off[-1]), w)).astype(dt)
+    plan = S.SignaturePlan(off, w, d, mode)
+    want = plan.run(torch.from_numpy(inc).cuda()).cpu()
+    inc_h = torch.from_numpy(inc).pin_memory()
+    out_h = torch.full((len(lens), plan.size), float("nan"), dtype=plan.dtype).pin_memory()
+    plan.run_host_pipelined(inc_h, out_h, n_chunks=chunks)
+    torch.cuda.synchronize()
+    assert torch.equal(out_h, want)
