@@ -541,6 +541,22 @@ def profile_slice(n):
     print("profile slice done", n)
 
 
+def profile_fma(w, d, batch):
+    """One float64 and one float32 C += A (x) B launch over `batch` pairs."""
+    import torch
+    from roughpy_b200 import _lib
+    T = int(_lib.lib.rpyb_tensor_size(w, d))
+    for dt, code in ((torch.float64, _lib.F64), (torch.float32, _lib.F32)):
+        g = torch.Generator(device="cuda").manual_seed(1)
+        A = torch.randn(batch, T, dtype=dt, device="cuda", generator=g)
+        B = torch.randn(batch, T, dtype=dt, device="cuda", generator=g)
+        C = torch.randn(batch, T, dtype=dt, device="cuda", generator=g)
+        _lib.check(_lib.lib.rpyb_ft_fma(code, w, d, batch, C.data_ptr(), A.data_ptr(),
+                                        B.data_ptr(), T, T, T, None, 0))
+        torch.cuda.synchronize()
+    print("profile fma done", w, d, batch)
+
+
 # ------------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
     """Reference CPU implementation of the path (rank 0 only)."""
@@ -623,9 +639,14 @@ def main():
                     help="skip the plain-f64, dyadic-query and backward workloads")
     ap.add_argument("--profile-slice", type=int, default=0,
                     help="run one launch per mode on an N-stream slice and exit")
+    ap.add_argument("--profile-fma", type=int, nargs=3, metavar=("WIDTH", "DEPTH", "BATCH"),
+                    help="run one float64 and one float32 FMA launch and exit")
     args = ap.parse_args()
     if args.profile_slice:
         profile_slice(args.profile_slice)
+        return
+    if args.profile_fma:
+        profile_fma(*args.profile_fma)
         return
     if args.warmup < 3 and args.impl == "b200":
         log("note: warmup raised to 3")

@@ -19,6 +19,7 @@
 #include "product.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace rpyb {
 namespace {
@@ -70,20 +71,38 @@ struct Acc<float> {
     __device__ __forceinline__ float value() const { return df_value(v); }
 };
 
-template <int D>
-__device__ __forceinline__ int64_t divd(int64_t x, int d)
-{
-    if constexpr (D > 0) {
-        return x / D;
-    } else {
-        return x / d;
-    }
-}
+// Alternative float32 accumulators (selected by RPYB_F32_ACC for measurement):
+// float64 accumulation of the exact float32 products, and plain float32 FMA.
+struct AccF32in64 {
+    double v;
+    __device__ __forceinline__ void init(float x) { v = (double)x; }
+    __device__ __forceinline__ void add(float a, float b) { v = fma((double)a, (double)b, v); }
+    __device__ __forceinline__ float value() const { return (float)v; }
+};
+struct AccF32Plain {
+    float v;
+    __device__ __forceinline__ void init(float x) { v = x; }
+    __device__ __forceinline__ void add(float a, float b) { v = fmaf(a, b, v); }
+    __device__ __forceinline__ float value() const { return v; }
+};
+
+template <typename T, int MODE>
+struct AccSel {
+    using type = Acc<T>;
+};
+template <>
+struct AccSel<float, 1> {
+    using type = AccF32in64;
+};
+template <>
+struct AccSel<float, 2> {
+    using type = AccF32Plain;
+};
 
 // T: output, left factor and accumulation type; TR: right factor type
 // (TR = float with T = double is the mixed mode: float32 right factors
 // accumulated into float64 rows).
-template <typename T, typename TR, int D>
+template <typename T, typename TR, int D, int ACC = 0>
 __global__ void __launch_bounds__(kThreads)
 product_kernel(const KArgs a)
 {
@@ -119,7 +138,7 @@ product_kernel(const KArgs a)
             const int64_t dk1 = a.pw[k - 1];
             const int64_t obase = a.db[k] + r;
 
-            Acc<T> acc[(D > 0) ? D : 16];
+            typename AccSel<T, ACC>::type acc[(D > 0) ? D : 16];
 #pragma unroll
             for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
                 if (D > 0 || u < d) {
@@ -130,29 +149,34 @@ product_kernel(const KArgs a)
             const int pmax = a.pmax[k];
             const int pmin = a.pmin[k];
             if (pmax >= pmin) {
-                // suffix length s = k - p, starting at the largest lhs degree
-                int s = k - pmax;
-                int64_t q = r / a.pw[s];
-                int64_t m = r - q * a.pw[s];
-                for (int p = pmax; p >= pmin; --p) {
-                    if (p == 0) {
-                        const TR* rk = rhs + a.db[k] + r;
+                // Walk the split points from p = k down (suffix length s = k - p
+                // growing), peeling one letter off the prefix q onto the suffix m
+                // per step; word indices fit in 32 bits, and with a compile-time
+                // width the division by d is a multiply-shift.
+                uint32_t q = (uint32_t)r;
+                uint32_t m = 0;
+                int s = 0;
+                for (int p = k; p >= pmin; --p) {
+                    if (p <= pmax) {
+                        if (p == 0) {
+                            const TR* rk = rhs + a.db[k] + r;
 #pragma unroll
-                        for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
-                            if (D > 0 || u < d) acc[u].add(lhs0, T(__ldg(rk + u * dk1)));
-                        }
-                    } else {
-                        const T rv = T(__ldg(rhs + a.db[s] + m));
-                        const T* lp = lhs + a.db[p] + q;
-                        const int64_t dp1 = a.pw[p - 1];
+                            for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
+                                if (D > 0 || u < d) acc[u].add(lhs0, T(__ldg(rk + u * dk1)));
+                            }
+                        } else {
+                            const T rv = T(__ldg(rhs + a.db[s] + m));
+                            const T* lp = lhs + a.db[p] + q;
+                            const uint32_t dp1 = (uint32_t)a.pw[p - 1];
 #pragma unroll
-                        for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
-                            if (D > 0 || u < d) acc[u].add(__ldg(lp + u * dp1), rv);
+                            for (int u = 0; u < ((D > 0) ? D : 16); ++u) {
+                                if (D > 0 || u < d) acc[u].add(__ldg(lp + u * dp1), rv);
+                            }
                         }
                     }
                     // advance to suffix length s + 1
-                    const int64_t q2 = divd<D>(q, d);
-                    m += (q - q2 * d) * a.pw[s];
+                    const uint32_t q2 = (D > 0) ? q / (uint32_t)D : q / (uint32_t)d;
+                    m += (q - q2 * (uint32_t)d) * (uint32_t)a.pw[s];
                     q = q2;
                     ++s;
                 }
@@ -190,24 +214,46 @@ __global__ void convert_rows_kernel(TD* dst, int64_t ld_dst, const TS* src, int6
     }
 }
 
-template <typename T, typename TR>
+template <typename T, typename TR, int ACC>
 int dispatch(const KArgs& a, dim3 grid, cudaStream_t stream)
 {
     switch (a.width) {
-        case 2: product_kernel<T, TR, 2><<<grid, kThreads, 0, stream>>>(a); break;
-        case 3: product_kernel<T, TR, 3><<<grid, kThreads, 0, stream>>>(a); break;
-        case 4: product_kernel<T, TR, 4><<<grid, kThreads, 0, stream>>>(a); break;
-        case 5: product_kernel<T, TR, 5><<<grid, kThreads, 0, stream>>>(a); break;
-        case 6: product_kernel<T, TR, 6><<<grid, kThreads, 0, stream>>>(a); break;
-        case 7: product_kernel<T, TR, 7><<<grid, kThreads, 0, stream>>>(a); break;
-        case 8: product_kernel<T, TR, 8><<<grid, kThreads, 0, stream>>>(a); break;
+        case 2: product_kernel<T, TR, 2, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 3: product_kernel<T, TR, 3, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 4: product_kernel<T, TR, 4, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 5: product_kernel<T, TR, 5, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6: product_kernel<T, TR, 6, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 7: product_kernel<T, TR, 7, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 8: product_kernel<T, TR, 8, ACC><<<grid, kThreads, 0, stream>>>(a); break;
         default:
             if (a.width > 16) return fail(RPYB_E_UNSUPPORTED, "product kernel supports width <= 16");
-            product_kernel<T, TR, 0><<<grid, kThreads, 0, stream>>>(a);
+            product_kernel<T, TR, 0, ACC><<<grid, kThreads, 0, stream>>>(a);
             break;
     }
     RPYB_CUDA(cudaGetLastError());
     return RPYB_OK;
+}
+
+int f32_acc_mode()
+{
+    static int m = [] {
+        const char* e = getenv("RPYB_F32_ACC");
+        if (!e) return 0;
+        if (e[0] == 'f') return 1;   // "f64"
+        if (e[0] == 'p') return 2;   // "plain"
+        return 0;
+    }();
+    return m;
+}
+
+int tile_words()
+{
+    static int w = [] {
+        const char* e = getenv("RPYB_TILE_WORDS");
+        int v = e ? atoi(e) : 4096;
+        return v >= 256 ? v : 4096;
+    }();
+    return w;
 }
 
 }  // namespace
@@ -257,15 +303,20 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
     a.rhs_idx = rows.rhs_idx;
     a.batch = rows.batch;
 
-    // Suffixes per tile: about 4096 output words per CTA (>= one per thread).
-    a.tile_r = std::max<int64_t>(kThreads, 4096 / std::max(1, g.width));
+    // Suffixes per tile: about kTileWords output words per CTA (at least one
+    // suffix per thread).
+    a.tile_r = std::max<int64_t>(kThreads, tile_words() / std::max(1, g.width));
     int64_t tiles = (a.ftotal + a.tile_r - 1) / a.tile_r;
     if (tiles == 0) tiles = 1;  // level 0 only
     if (tiles > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "tensor too large");
     dim3 grid((unsigned)tiles, (unsigned)std::min<int64_t>(rows.batch, 65535), 1);
-    if (dtype == RPYB_F64) return dispatch<double, double>(a, grid, stream);
-    if (dtype == kMixedF64F32) return dispatch<double, float>(a, grid, stream);
-    return dispatch<float, float>(a, grid, stream);
+    if (dtype == RPYB_F64) return dispatch<double, double, 0>(a, grid, stream);
+    if (dtype == kMixedF64F32) return dispatch<double, float, 0>(a, grid, stream);
+    switch (f32_acc_mode()) {
+        case 1: return dispatch<float, float, 1>(a, grid, stream);
+        case 2: return dispatch<float, float, 2>(a, grid, stream);
+        default: return dispatch<float, float, 0>(a, grid, stream);
+    }
 }
 
 int launch_convert_rows(int dst_dtype, void* dst, int64_t ld_dst, int src_dtype,
