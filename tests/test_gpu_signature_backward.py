@@ -34,7 +34,10 @@ def torch_signature(inc, width, depth):
 
 
 @pytest.mark.parametrize("w,d,lens,K", [(2, 3, [7, 1, 0, 12], 4), (3, 4, [20, 33], 64),
-                                        (4, 3, [9, 16], 1), (5, 2, [11], 3)])
+                                        (4, 3, [9, 16], 1), (5, 2, [11], 3),
+                                        (2, 5, [9, 4, 70], 8), (3, 5, [6, 40], 16),
+                                        (8, 5, [3, 5], 2), (2, 8, [5, 37], 64),
+                                        (4, 6, [4, 1], 3), (6, 6, [3], 2), (3, 1, [5, 2], 2)])
 def test_f64_gradient_equals_autograd(w, d, lens, K):
     rng = np.random.default_rng(w + 10 * d)
     off = S.offsets_from_lengths(lens)
@@ -57,6 +60,22 @@ def test_f64_gradient_equals_autograd(w, d, lens, K):
     ref_sig = torch.stack([torch_signature(inc[off[s]:off[s + 1]], w, d)
                            for s in range(len(lens))])
     assert float((sig.detach() - ref_sig).abs().max()) <= 1e-12 * float(ref_sig.abs().max())
+
+
+@pytest.mark.parametrize("w,d", [(8, 5), (3, 5), (2, 2)])
+def test_f32_gradient_against_f64(w, d):
+    rng = np.random.default_rng(100 + w * d)
+    lens = [50, 7, 130]
+    off = S.offsets_from_lengths(lens)
+    inc = torch.from_numpy(rng.normal(0, 0.2, size=(int(off[-1]), w))).cuda()
+    T = S.tensor_size(w, d)
+    W = torch.from_numpy(rng.normal(size=(len(lens), T))).cuda()
+    x32 = inc.float().clone().requires_grad_(True)
+    (S.signature_with_grad(x32, S.SignaturePlan(off, w, d, "f32c")).double() * W).sum().backward()
+    x64 = inc.float().double().clone().requires_grad_(True)
+    (S.signature_with_grad(x64, S.SignaturePlan(off, w, d, "f64")) * W).sum().backward()
+    err = float((x32.grad.double() - x64.grad).abs().max()) / float(x64.grad.abs().max())
+    assert err <= 1e-5, err
 
 
 def test_config5_shape_finite_differences_and_f32():
