@@ -523,7 +523,47 @@ def signature_backward(dev):
     g64 = grads["f64"]
     res["f32c_grad_max_rel_err_vs_f64"] = float((grads["f32c"] - g64).abs().max() /
                                                 g64.abs().max())
+    # the adjoint kernel alone (one launch over all streams)
+    for mode, dt in (("f32c", torch.float32), ("f64", torch.float64)):
+        launch = _backward_launch(mode, dt, n, L, w, d, inc, W, dev)
+        res[mode]["ms_backward_kernel"] = round(_events_time(torch, launch, 3, warm=1), 3)
     return res
+
+
+def _backward_launch(mode, dt, n, L, w, d, inc, W, dev):
+    """A closure running rpyb_signature_backward once on the given batch."""
+    import torch
+    from roughpy_b200 import _lib
+    from roughpy_b200 import signatures as S
+    off = np.arange(n + 1, dtype=np.int64) * L
+    plan = S.SignaturePlan(off, w, d, mode, device=dev)
+    x = torch.from_numpy(inc[:n * L]).to(dev, dt)
+    G = W.to(dt).expand(n, plan.size).contiguous()
+    ws = int(_lib.lib.rpyb_signature_backward_workspace_size(plan.code, w, d, n, L, 64))
+    wsb = torch.empty(max(ws, 1), dtype=torch.uint8, device=dev)
+    gi = torch.empty_like(x)
+
+    def launch():
+        _lib.check(_lib.lib.rpyb_signature_backward(
+            plan.code, w, d, n, plan.offsets.data_ptr(), L, x.data_ptr(), G.data_ptr(),
+            G.stride(0), gi.data_ptr(), 64, wsb.data_ptr(), ws,
+            torch.cuda.current_stream(dev).cuda_stream))
+        return gi
+    return launch
+
+
+def profile_backward(n):
+    """One f32c adjoint launch on the first n streams of the 512 x 1024,
+    width 5, depth 6 backward workload (the case captured by ncu)."""
+    import torch
+    L, w, d = 1024, 5, 6
+    rng = np.random.default_rng(4)
+    inc = rng.normal(0, np.sqrt(1.0 / L), size=(512 * L, w))
+    T = (w ** (d + 1) - 1) // (w - 1)
+    W = torch.from_numpy(rng.normal(size=(T,))).cuda()
+    _backward_launch("f32c", torch.float32, n, L, w, d, inc, W, torch.device("cuda"))()
+    torch.cuda.synchronize()
+    print("profile backward done", n)
 
 
 def profile_slice(n):
@@ -637,11 +677,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the plain-f64, dyadic-query and backward workloads")
+    ap.add_argument("--profile-backward", type=int, default=0,
+                    help="run one adjoint launch on N streams of the backward workload and exit")
     ap.add_argument("--profile-slice", type=int, default=0,
                     help="run one launch per mode on an N-stream slice and exit")
     ap.add_argument("--profile-fma", type=int, nargs=3, metavar=("WIDTH", "DEPTH", "BATCH"),
                     help="run one float64 and one float32 FMA launch and exit")
     args = ap.parse_args()
+    if args.profile_backward:
+        profile_backward(args.profile_backward)
+        return
     if args.profile_slice:
         profile_slice(args.profile_slice)
         return
