@@ -240,12 +240,14 @@ RPYB_API int rpyb_signature_host(int mode, int32_t width, int32_t depth, int64_t
  * Reverse-mode derivative of rpyb_signature: given the upstream gradient
  * grad_sig (dLoss/dS per stream, [n_streams, T] with row stride ld_grad, or
  * one shared row when ld_grad == 0), writes grad_inc = dLoss/d increments
- * ([total, width]).  One block per stream walks it backwards: the states are
- * checkpointed every `checkpoint_every` steps by a float64 forward pass and
- * recomputed per segment; each step is differentiated through its Horner
- * chains (reverse Chen products).  The gradient accumulator is float64 in
- * both modes.  `max_len` must bound every stream length (it sizes the
- * checkpoint scratch); longer streams get NaN gradients.  Width <= 8.
+ * ([total, width]).  One block per stream walks it backwards, propagating
+ * the adjoint G_t = exp(D_x) G_{t+1} (the reverse Chen product) and the
+ * increment gradients; states are recovered by inverse steps re-anchored on
+ * float64 checkpoints every `checkpoint_every` steps (widths 2..8 with
+ * width^(depth-2) <= 992), or recomputed per segment from them (other
+ * shapes).  Adjoint accumulators are float64 in both modes.  `max_len` must
+ * bound every stream length (it sizes the checkpoint scratch); longer streams
+ * get NaN gradients.  Width <= 8.
  * No reference counterpart: RoughPy only has the forward-mode derivative
  * (algebra/src/lite_context.h:577-636, LiteContext::sig_derivative_impl).
  */
@@ -280,8 +282,10 @@ RPYB_API int64_t rpyb_lie_map_csr(int32_t width, int32_t depth, int which,
                                   int64_t* indptr, int64_t* indices, double* values);
 
 /*
- * y[b] = scale * M x[b] for a CSR matrix M (device arrays, float64 values),
+ * y[b] += scale * M x[b] for a CSR matrix M (device arrays, float64 values),
  * batched over rows; x, y of dtype (float32 rows are computed in float64).
+ * The map accumulates into y, as the reference's does: zero y for a plain
+ * product.
  * Replaces: roughpy_compute/dense/basic/apply_sparse_linear_map.hpp:16-55 via
  *           roughpy/compute/_src/dense_basic.cpp:564-620 and :1055-1150.
  */
@@ -304,6 +308,57 @@ RPYB_API int64_t rpyb_dyadic_dissect(double inf, double sup, int32_t tol, int cl
 RPYB_API int rpyb_dyadic_dissect_batch(int64_t n, const double* inf, const double* sup,
                                        const int32_t* tol, int clopen, int64_t* k,
                                        int32_t* p, int64_t cap, int64_t* offsets);
+
+/*
+ * Dyadic signature tree of a stream of Lie increments (opaque, device-
+ * resident), and batched interval queries against it.
+ *
+ * rpyb_dyadic_build: events e < n_events at non-decreasing times_host[e]
+ * (host array) carry device rows `rows` ([n_events, row_len], float64 for
+ * RPYB_F64, float32 for RPYB_F32): level-1 increments (row_len == width) or
+ * Hall-basis Lie coordinates (row_len == rpyb_lie_basis_size).  Leaves are the
+ * dyadic intervals of `resolution` meeting the support [support_inf,
+ * support_sup) and the event times; each leaf is the Chen product of exp over
+ * its events, and every coarser aligned dyadic block is the product of its
+ * halves.  The handle owns its device memory (allocated on the current
+ * device, released by rpyb_dyadic_free); the build is ordered on `stream`.
+ * Replaces: the LieIncrementStream constructor and the DyadicCachingLayer
+ * cache (streams/src/lie_increment_stream.cpp:116-199,
+ * streams/src/dyadic_caching_layer.cpp:86-154), which cache leaves only and
+ * recompute coarser pieces by recursive CBH.
+ *
+ * rpyb_dyadic_query: for each clopen query [inf_host[q], sup_host[q]) (host
+ * arrays; inf <= sup), trims to the support, dissects at `resolution`
+ * (RPYB_QUERY_RESOLUTION_AUTO: the reference's per-query choice
+ * max(stream resolution, query_resolution(length) + 2)), multiplies the
+ * pieces' node signatures in order in float64 and writes the log-signature
+ * in Hall coordinates (out_logsig, [n, ld_logsig], device float64) and/or
+ * the signature exp(l2t(logsig)) (out_sig, [n, ld_sig]); either may be NULL.
+ * Thread-safe on a built tree; temporaries are stream-ordered allocations.
+ * Replaces: Stream::log_signature / Stream::signature
+ * (streams/src/stream.cpp:54-171) with intervals/src/dyadic_interval.cpp:191-224
+ * and algebra/src/context.cpp:156-215.
+ *
+ * rpyb_dyadic_tree_info / rpyb_dyadic_node_row expose the node table (rows of
+ * tensor_size values of the mode's type) for inspection; node_row returns the
+ * row of dyadic block `block` at `level` levels above the leaves (the
+ * interval [block, block+1) * 2^(level - resolution)), or -1.
+ */
+typedef struct rpyb_dyadic_tree rpyb_dyadic_tree;
+#define RPYB_QUERY_RESOLUTION_AUTO (-2147483647 - 1)
+RPYB_API int rpyb_dyadic_build(int mode, int32_t width, int32_t depth, int32_t resolution,
+                               double support_inf, double support_sup, int64_t n_events,
+                               const double* times_host, const void* rows, int32_t row_len,
+                               rpyb_dyadic_tree** tree, void* stream);
+RPYB_API int rpyb_dyadic_free(rpyb_dyadic_tree* tree);
+RPYB_API int rpyb_dyadic_tree_info(const rpyb_dyadic_tree* tree, int64_t* rows,
+                                   int32_t* top_level, const void** nodes);
+RPYB_API int64_t rpyb_dyadic_node_row(const rpyb_dyadic_tree* tree, int32_t level,
+                                      int64_t block);
+RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* tree, int64_t n_queries,
+                               const double* inf_host, const double* sup_host,
+                               int32_t resolution, double* out_logsig, int64_t ld_logsig,
+                               double* out_sig, int64_t ld_sig, void* stream);
 
 #ifdef __cplusplus
 }

@@ -81,7 +81,16 @@ SIGNATURES = {
                                _vp]),
     "rpyb_dyadic_dissect": (_i64, [_dbl, _dbl, _i32, _int, _vp, _vp, _i64]),
     "rpyb_dyadic_dissect_batch": (_int, [_i64, _vp, _vp, _vp, _int, _vp, _vp, _i64, _vp]),
+    "rpyb_dyadic_build": (_int, [_int, _i32, _i32, _i32, _dbl, _dbl, _i64, _vp, _vp, _i32, _vp,
+                                 _vp]),
+    "rpyb_dyadic_free": (_int, [_vp]),
+    "rpyb_dyadic_tree_info": (_int, [_vp, _vp, _vp, _vp]),
+    "rpyb_dyadic_node_row": (_i64, [_vp, _i32, _i64]),
+    "rpyb_dyadic_query": (_int, [_vp, _i64, _vp, _vp, _i32, _vp, _i64, _vp, _i64, _vp]),
 }
+
+# rpyb_dyadic_query: choose the dissection resolution per query as the reference does
+QUERY_RESOLUTION_AUTO = -2147483648
 
 for _name, (_res, _args) in SIGNATURES.items():
     _f = getattr(lib, _name)

@@ -84,6 +84,12 @@ class SignaturePlan:
             raise ValueError("increments do not match the offsets")
         if out is None:
             out = torch.empty((self.n_streams, self.size), dtype=self.dtype, device=self.device)
+        if self.total == 0:
+            # every stream is empty: the signatures are unit tensors
+            with torch.cuda.stream(stream or torch.cuda.current_stream(self.device)):
+                out.zero_()
+                out[:, 0] = 1.0
+            return out
         s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
         _lib.check(_lib.lib.rpyb_signature(
             self.code, self.width, self.depth, self.n_streams, self.offsets.data_ptr(),

@@ -21,14 +21,17 @@ streams/src/dyadic_caching_layer.cpp:86-154, algebra/src/context.cpp:156-215):
 
 B200 design.  The reference caches only the leaves and recomputes every coarser
 piece by recursive CBH at query time.  Here the whole dyadic tree is built once
-on the GPU: leaf signatures come from the batched signature kernel (level-1
-increments) or from exp of the embedded Lie increments (general increments),
-and every coarser node is the product of its children (one batched product
-launch per level).  A query is then the ordered product of at most ~2 x
-resolution cached node signatures (batched across queries, one launch per
-piece position), followed by a float64 log and the Lie projection.  Since
-``log``/``exp`` are mutually inverse on group-like elements and CBH is
-associative, this equals the reference's CBH recursion up to rounding.
+on the GPU by the native runtime behind the C ABI (``rpyb_dyadic_build``): leaf
+signatures come from the batched signature kernel (level-1 increments) or from
+exp of the embedded Lie increments (general increments), and every coarser node
+is the product of its children (one batched product launch per level).  A query
+batch (``rpyb_dyadic_query``) is trimmed and dissected on the host, then each
+query is the ordered product of at most ~2 x resolution cached node signatures
+(batched across queries, one launch per piece position), followed by a float64
+log and the Lie projection.  Since ``log``/``exp`` are mutually inverse on
+group-like elements and CBH is associative, this equals the reference's CBH
+recursion up to rounding.  This module keeps the reference's construction
+rules (event de-duplication, the resolution heuristic, the default support).
 """
 from __future__ import annotations
 
@@ -213,193 +216,58 @@ class LieIncrementStream:
         return torch.float64 if self.mode == "f64" else torch.float32
 
     def _build_tree(self):
-        """All dyadic nodes at and above the stream resolution, on the GPU.
-
-        Level j holds the aligned blocks of 2^j leaves intersecting the leaf
-        range [m_lo, m_hi]: block b covers leaves [b 2^j, (b+1) 2^j), which is
-        the dyadic interval (b, resolution - j).  Block ranges follow floor
-        division, so supports on both sides of 0 (where no dyadic interval
-        spans the origin) work too.  The last row of the tree is the unit,
-        standing in for children outside the range.
-        """
+        """The device dyadic tree (``rpyb_dyadic_build``), built on first use."""
         if self._tree is not None:
             return self._tree
-        R = self.resolution
-        s0, s1 = self.support.inf, self.support.sup
-        m_lo = math.floor(math.ldexp(s0, R))
-        m_hi = max(m_lo, math.ceil(math.ldexp(s1, R)) - 1)
-        if self.times.size:
-            m_lo = min(m_lo, math.floor(math.ldexp(float(self.times.min()), R)))
-            m_hi = max(m_hi, math.floor(math.ldexp(float(self.times.max()), R)))
-        lo, cnt, base = [], [], []
-        rows = 0
-        j = 0
-        while True:
-            l_j, h_j = m_lo >> j, m_hi >> j
-            # a range on both sides of 0 stops merging at blocks -1 and 0
-            if j > 0 and l_j == -1 and h_j == 0 and cnt[-1] == 2:
-                break
-            lo.append(l_j)
-            cnt.append(h_j - l_j + 1)
-            base.append(rows)
-            rows += h_j - l_j + 1
-            if h_j == l_j:
-                break
-            j += 1
-            if j > 62:
-                raise ValueError("stream support too wide for its resolution")
-        J = len(lo) - 1
-        unit_row = rows
-        rows += 1
-        T = self.tensor_basis.size()
         dt = self._sig_dtype
-        dev = self.device
         code = _lib.F64 if dt == torch.float64 else _lib.F32
-        tree = torch.empty((rows, T), dtype=dt, device=dev)
-        tree[unit_row].zero_()
-        tree[unit_row, 0] = 1.0
-        # leaves: events grouped by leaf, Chen product of exp(increment)
-        n_leaves = cnt[0]
-        leaf_of = np.floor(np.ldexp(self.times, R)).astype(np.int64) - m_lo
-        off = np.searchsorted(leaf_of, np.arange(n_leaves + 1), side="left").astype(np.int64)
-        leaves = tree[:n_leaves]
         higher = self.lies[:, self.width:]
         if higher.size == 0 or not np.any(higher):
-            inc = torch.from_numpy(np.ascontiguousarray(self.lies[:, :self.width])).to(dev, dt)
-            plan = S.SignaturePlan(off, self.width, self.depth, self.mode, device=dev)
-            plan.run(inc.contiguous(), leaves)
+            rows, row_len = self.lies[:, :self.width], self.width
         else:
-            self._general_leaves(leaves, off, code)
-        # level j node b = child (j-1, 2b) * child (j-1, 2b+1)
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        for j in range(1, J + 1):
-            b = np.arange(lo[j], lo[j] + cnt[j], dtype=np.int64)
-            kids = []
-            for c in (2 * b, 2 * b + 1):
-                inside = (c >= lo[j - 1]) & (c < lo[j - 1] + cnt[j - 1])
-                kids.append(np.where(inside, base[j - 1] + (c - lo[j - 1]), unit_row))
-            out_idx = torch.from_numpy(base[j] + (b - lo[j])).to(dev)
-            lhs_idx = torch.from_numpy(kids[0]).to(dev)
-            rhs_idx = torch.from_numpy(kids[1]).to(dev)
-            _lib.check(_lib.lib.rpyb_ft_mul_gather(
-                code, self.width, self.depth, cnt[j], tree.data_ptr(), tree.data_ptr(),
-                tree.data_ptr(), T, out_idx.data_ptr(), lhs_idx.data_ptr(),
-                rhs_idx.data_ptr(), 0, stream))
-        self._tree = dict(tensor=tree, J=J, lo=lo, cnt=cnt, base=base, unit_row=unit_row)
+            rows, row_len = self.lies, self.lies.shape[1]
+        n = int(self.times.shape[0])
+        rows_t = torch.from_numpy(np.ascontiguousarray(rows)).to(self.device, dt).contiguous()
+        times = np.ascontiguousarray(self.times, dtype=np.float64)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(_lib.lib.rpyb_dyadic_build(
+                code, self.width, self.depth, self.resolution, float(self.support.inf),
+                float(self.support.sup), n, times.ctypes.data if n else None,
+                rows_t.data_ptr() if n else None, row_len, ctypes.byref(handle), stream))
+        self._tree = _DyadicTree(handle, self.device)
         return self._tree
 
-    def _general_leaves(self, leaves, off, code):
-        """Leaves for increments with higher Hall coordinates: Π exp(l2t(lie))."""
-        dev = self.device
-        dt = leaves.dtype
-        T = self.tensor_basis.size()
-        l2t = self.lie_basis.get_l2t_matrix()
-        lies = torch.from_numpy(np.ascontiguousarray(self.lies)).to(dev, dt)
-        emb = torch.zeros((lies.shape[0], T), dtype=dt, device=dev)
-        if lies.shape[0]:
-            rpc._internals.dense_lie_to_tensor(emb, lies, l2t, self.lie_basis, self.tensor_basis)
-        ex = torch.zeros_like(emb)
-        if lies.shape[0]:
-            rpc._internals.dense_ft_exp(ex, emb, self.tensor_basis)
-        counts = np.diff(off)
-        leaves.zero_()
-        leaves[:, 0] = 1.0
-        _ordered_products(leaves, ex, off, counts, code, self.width, self.depth)
-
     # ------------------------------------------------------------- queries
-    def _pieces(self, infs, sups, resolution):
-        """Per query: node rows of the tree, in order (zero pieces dropped)."""
+    def _query(self, infs, sups, resolution, logsig=True, sig=False):
+        """One rpyb_dyadic_query over clopen intervals; float64 device outputs."""
         tr = self._build_tree()
-        R, J = self.resolution, tr["J"]
-        s0, s1 = self.support.inf, self.support.sup
-        n = len(infs)
-        qi = np.empty(n)
-        qs = np.empty(n)
-        tols = np.empty(n, dtype=np.int32)
-        empty = np.zeros(n, dtype=bool)
-        for q in range(n):
-            a, b = float(infs[q]), float(sups[q])
-            if a > b:
-                raise ValueError("inf must not be larger than sup")
-            # stream.cpp:37-52 check_support_and_trim, :54-71 refine_interval
-            if b < s0 or a > s1:
-                empty[q] = True
-                a = b = s0
-            else:
-                a, b = max(a, s0), min(b, s1)
-            if b - a == 0.0:
-                empty[q] = True
-            qi[q], qs[q] = a, b
-            if resolution is None:
-                tols[q] = max(R, _query_param_to_resolution(b - a) + 2) if not empty[q] else R
-            else:
-                tols[q] = int(resolution)
-        k, p, off = _dissect_batch(qi, qs, tols)
-        nodes = np.full(k.shape[0], -1, dtype=np.int64)
-        lo = np.asarray(tr["lo"], dtype=np.int64)
-        cnt = np.asarray(tr["cnt"], dtype=np.int64)
-        base = np.asarray(tr["base"], dtype=np.int64)
-
-        def node_rows(level, blk):
-            ok = (level >= 0) & (level <= J)
-            lv = np.clip(level, 0, J)
-            rel = blk - lo[lv]
-            ok &= (rel >= 0) & (rel < cnt[lv])
-            return np.where(ok, base[lv] + rel, -1)
-
-        # dyadic_caching_layer.cpp:86-130: at the stream resolution a cached leaf;
-        # coarser pieces are whole tree nodes (the CBH of their halves); a finer
-        # piece maps to the leaf it starts in when the start points coincide
-        # (rational_equals on the included ends) and is dropped otherwise.
-        at = p <= R
-        nodes[at] = node_rows((R - p[at]).astype(np.int64), k[at])
-        fine = p > R
-        if np.any(fine):
-            sh = (p[fine] - R).astype(np.int64)
-            kk = k[fine]
-            tk = kk >> sh
-            same = (tk << sh) == kk
-            nodes[fine] = np.where(same, node_rows(np.zeros_like(tk), tk), -1)
-        for q in np.nonzero(empty)[0]:
-            nodes[off[q]:off[q + 1]] = -1
-        return nodes, off
-
-    def _query_products(self, infs, sups, resolution):
-        tr = self._build_tree()
-        tree = tr["tensor"]
-        nodes, off = self._pieces(infs, sups, resolution)
-        n = len(infs)
-        # drop zero pieces, keep order
-        keep = nodes >= 0
-        cs = np.zeros(nodes.shape[0] + 1, dtype=np.int64)
-        np.cumsum(keep, out=cs[1:])
-        counts = cs[off[1:]] - cs[off[:-1]]
-        kept = nodes[keep]
-        koff = np.zeros(n + 1, dtype=np.int64)
-        np.cumsum(counts, out=koff[1:])
-        T = self.tensor_basis.size()
-        # queries accumulate in float64; float32 nodes enter through the mixed product
-        acc = torch.zeros((n, T), dtype=torch.float64, device=self.device)
-        acc[:, 0] = 1.0
-        _ordered_products(acc, tree, koff, counts, None, self.width, self.depth, src_rows=kept)
-        return acc
+        infs = np.ascontiguousarray(infs, dtype=np.float64).reshape(-1)
+        sups = np.ascontiguousarray(sups, dtype=np.float64).reshape(-1)
+        n = infs.shape[0]
+        L, T = self.lie_basis.size(), self.tensor_basis.size()
+        lie = torch.empty((n, L), dtype=torch.float64, device=self.device) if logsig else None
+        sg = torch.empty((n, T), dtype=torch.float64, device=self.device) if sig else None
+        if n == 0:
+            return lie, sg
+        res = _lib.QUERY_RESOLUTION_AUTO if resolution is None else int(resolution)
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(_lib.lib.rpyb_dyadic_query(
+                tr.handle, n, infs.ctypes.data, sups.ctypes.data, res,
+                lie.data_ptr() if logsig else None, L, sg.data_ptr() if sig else None, T,
+                stream))
+        return lie, sg
 
     def _log_signature_batch(self, infs, sups, resolution=None):
-        prods = self._query_products(infs, sups, resolution)
-        p64 = prods
-        logs = torch.zeros_like(p64)
-        rpc._internals.dense_ft_log(logs, p64, self.tensor_basis)
-        lie = torch.zeros((p64.shape[0], self.lie_basis.size()), dtype=torch.float64,
-                          device=self.device)
-        rpc._internals.dense_tensor_to_lie(lie, logs, self.lie_basis.get_t2l_matrix(),
-                                           self.lie_basis, self.tensor_basis)
-        return lie
+        return self._query(infs, sups, resolution)[0]
 
     def log_signature_batch(self, infs, sups, resolution=None, chunk=16384):
         """Log-signatures (Hall coordinates, float64) of many clopen intervals."""
         infs = np.asarray(infs, dtype=np.float64).reshape(-1)
         sups = np.asarray(sups, dtype=np.float64).reshape(-1)
-        outs = [self._log_signature_batch(infs[i:i + chunk], sups[i:i + chunk], resolution)
+        outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution)[0]
                 for i in range(0, infs.shape[0], chunk)]
         if not outs:
             return torch.zeros((0, self.lie_basis.size()), dtype=torch.float64, device=self.device)
@@ -407,18 +275,14 @@ class LieIncrementStream:
 
     def signature_batch(self, infs, sups, resolution=None, chunk=16384):
         """Signatures exp(l2t(log_signature)) (float64) of many clopen intervals."""
-        lie = self.log_signature_batch(infs, sups, resolution, chunk)
-        return self._to_signature(lie)
-
-    def _to_signature(self, lie):
-        # algebra/src/context.cpp:156-159: exp(lie_to_tensor(log_signature))
-        T = self.tensor_basis.size()
-        emb = torch.zeros((lie.shape[0], T), dtype=torch.float64, device=self.device)
-        rpc._internals.dense_lie_to_tensor(emb, lie, self.lie_basis.get_l2t_matrix(),
-                                           self.lie_basis, self.tensor_basis)
-        sig = torch.zeros_like(emb)
-        rpc._internals.dense_ft_exp(sig, emb, self.tensor_basis)
-        return sig
+        infs = np.asarray(infs, dtype=np.float64).reshape(-1)
+        sups = np.asarray(sups, dtype=np.float64).reshape(-1)
+        outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution, False, True)[1]
+                for i in range(0, infs.shape[0], chunk)]
+        if not outs:
+            return torch.zeros((0, self.tensor_basis.size()), dtype=torch.float64,
+                               device=self.device)
+        return torch.cat(outs)
 
     def _interval_args(self, interval_or_inf, sup):
         if interval_or_inf is None:
@@ -450,46 +314,32 @@ class LieIncrementStream:
     def signature(self, interval_or_inf=None, sup=None, resolution=None, depth=None):
         """Signature over an interval (streams/src/stream.cpp:156-171), float64 numpy."""
         a, b = self._interval_args(interval_or_inf, sup)
-        lie = self._log_signature_batch(np.array([a]), np.array([b]), resolution)
-        return self._truncate_tensor(self._to_signature(lie)[0].cpu().numpy(), depth)
+        sig = self._query(np.array([a]), np.array([b]), resolution, False, True)[1]
+        return self._truncate_tensor(sig[0].cpu().numpy(), depth)
 
 
-def _ordered_products(acc, src, off, counts, code, width, depth, src_rows=None):
-    """acc[q] <- acc[q] * src[r_0] * src[r_1] * ... over q's rows (in order).
+class _DyadicTree:
+    """Owner of an rpyb_dyadic_tree handle (device memory freed with it)."""
 
-    Rows of q are src_rows[off[q]:off[q+1]] (or the range itself when
-    src_rows is None).  One batched product launch per position.
-    """
-    n = acc.shape[0]
-    if n == 0:
-        return
-    dev = acc.device
-    T = acc.shape[1]
-    counts = np.asarray(counts, dtype=np.int64)
-    maxc = int(counts.max()) if counts.size else 0
-    if src_rows is None:
-        src_rows = np.arange(int(off[-1]), dtype=np.int64)
-    mixed = acc.dtype == torch.float64 and src.dtype == torch.float32
-    if not mixed and acc.dtype != src.dtype:
-        raise TypeError("unsupported dtype combination")
-    if code is None:
-        code = _lib.F64 if acc.dtype == torch.float64 else _lib.F32
-    tmp = torch.empty_like(acc)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    for r in range(maxc):
-        active = np.nonzero(counts > r)[0]
-        m = active.shape[0]
-        rows = src_rows[off[active] + r]
-        q_t = torch.from_numpy(active.astype(np.int64)).to(dev)
-        out_t = torch.arange(m, device=dev, dtype=torch.int64)
-        r_t = torch.from_numpy(rows).to(dev)
-        if mixed:
-            rc = _lib.lib.rpyb_ft_mul_gather_mixed(width, depth, m, tmp.data_ptr(), acc.data_ptr(),
-                                                   src.data_ptr(), T, out_t.data_ptr(),
-                                                   q_t.data_ptr(), r_t.data_ptr(), 0, stream)
-        else:
-            rc = _lib.lib.rpyb_ft_mul_gather(code, width, depth, m, tmp.data_ptr(),
-                                             acc.data_ptr(), src.data_ptr(), T, out_t.data_ptr(),
-                                             q_t.data_ptr(), r_t.data_ptr(), 0, stream)
-        _lib.check(rc)
-        acc.index_copy_(0, q_t, tmp[:m])
+    def __init__(self, handle, device):
+        self.handle = handle
+        self.device = device
+        rows = ctypes.c_int64()
+        top = ctypes.c_int32()
+        nodes = ctypes.c_void_p()
+        _lib.check(_lib.lib.rpyb_dyadic_tree_info(handle, ctypes.byref(rows), ctypes.byref(top),
+                                                  ctypes.byref(nodes)))
+        self.rows, self.top_level, self.nodes = rows.value, top.value, nodes.value
+
+    def node_row(self, level: int, block: int) -> int:
+        return int(_lib.lib.rpyb_dyadic_node_row(self.handle, int(level), int(block)))
+
+    def __del__(self):
+        h, self.handle = getattr(self, "handle", None), None
+        if h is not None and h.value:
+            try:
+                torch.cuda.current_stream(self.device).synchronize()
+                _lib.lib.rpyb_dyadic_free(h)
+            except Exception:
+                pass
+

@@ -152,3 +152,125 @@ def test_dyadic_queries_float32_tree_within_1e6():
     ref = s64b.signature_batch(q[:, 0], q[:, 1]).cpu().numpy()
     assert level_rel_err(sig32, ref, 6, 5) <= 1e-6
     assert sig64.shape == sig32.shape
+
+
+def _build_raw(mode, w, d, res, s0, s1, times, rows):
+    """rpyb_dyadic_build called directly through the C ABI."""
+    import ctypes
+    import torch
+    from roughpy_b200 import _lib
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib.rpyb_dyadic_build(mode, w, d, res, s0, s1, len(times),
+                                          times.ctypes.data, rows.data_ptr(), rows.shape[1],
+                                          ctypes.byref(h), torch.cuda.current_stream().cuda_stream))
+    return h
+
+
+def test_c_abi_tree_nodes_are_chen_products_of_their_leaves():
+    """Every node of rpyb_dyadic_build's tree equals the signature of the events
+    inside its dyadic interval (computed by the batched signature kernel), and
+    the top node over a support inside [0, 1) is the whole stream's signature."""
+    import ctypes
+    import torch
+    from roughpy_b200 import _lib
+    from roughpy_b200 import signatures as S
+    rng = np.random.default_rng(11)
+    w, d, res, n = 3, 4, 4, 37
+    times = np.sort(rng.uniform(0, 1, n))
+    inc = torch.from_numpy(rng.normal(0, 0.3, (n, w))).cuda()
+    h = _build_raw(_lib.F64, w, d, res, 0.0, 1.0, times, inc)
+    try:
+        rows, top, nodes = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_void_p()
+        _lib.check(_lib.lib.rpyb_dyadic_tree_info(h, ctypes.byref(rows), ctypes.byref(top),
+                                                  ctypes.byref(nodes)))
+        T = S.tensor_size(w, d)
+        assert top.value == res
+        for level in range(res + 1):
+            for blk in range(2 ** (res - level)):
+                r = int(_lib.lib.rpyb_dyadic_node_row(h, level, blk))
+                assert r >= 0
+                lo, hi = blk * 2.0 ** (level - res), (blk + 1) * 2.0 ** (level - res)
+                sel = (times >= lo) & (times < hi)
+                want = S.signature(inc[torch.from_numpy(sel).cuda()], None, d, "f64")[0]
+                torch.cuda.synchronize()
+                got = _node(nodes.value, r, T)
+                assert level_rel_err(got, want.cpu().numpy(), w, d) <= 1e-13
+        assert int(_lib.lib.rpyb_dyadic_node_row(h, res + 1, 0)) == -1
+        assert int(_lib.lib.rpyb_dyadic_node_row(h, 0, 2 ** res)) == -1
+    finally:
+        _lib.lib.rpyb_dyadic_free(h)
+
+
+def _node(ptr, row, T):
+    """Copy one float64 tree row from device memory to the host."""
+    import ctypes
+    from roughpy_b200 import _lib
+    host = np.empty(T, dtype=np.float64)
+    # cudaMemcpy resolved through librpyb's own CUDA runtime dependency
+    copy = _lib.lib.cudaMemcpy
+    copy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    copy.restype = ctypes.c_int
+    assert copy(host.ctypes.data, ptr + row * T * 8, T * 8, 2) == 0   # device to host
+    return host
+
+
+def test_c_abi_query_outputs_agree_and_reject_bad_intervals():
+    """rpyb_dyadic_query: log-signature alone, signature alone and both at once
+    agree; the signature is exp(l2t(logsig)); an interval with inf > sup is
+    rejected with RPYB_E_INVALID."""
+    import torch
+    from roughpy_b200 import _lib
+    from roughpy_b200 import compute as rpc
+    rng = np.random.default_rng(12)
+    w, d, res, n = 2, 5, 6, 90
+    times = np.sort(rng.uniform(-0.5, 1.5, n))
+    inc = torch.from_numpy(rng.normal(0, 0.2, (n, w))).cuda()
+    h = _build_raw(_lib.F64, w, d, res, -0.5, 1.5, times, inc)
+    try:
+        q = np.sort(rng.uniform(-0.7, 1.7, (25, 2)), axis=1)
+        a, b = np.ascontiguousarray(q[:, 0]), np.ascontiguousarray(q[:, 1])
+        L, T = rpc.LieBasis(w, d).size(), rpc.TensorBasis(w, d).size()
+        s = torch.cuda.current_stream().cuda_stream
+        l1 = torch.empty((25, L), dtype=torch.float64, device="cuda")
+        s1 = torch.empty((25, T + 3), dtype=torch.float64, device="cuda")
+        l2 = torch.empty_like(l1)
+        s2 = torch.empty((25, T), dtype=torch.float64, device="cuda")
+        A = _lib.QUERY_RESOLUTION_AUTO
+        _lib.check(_lib.lib.rpyb_dyadic_query(h, 25, a.ctypes.data, b.ctypes.data, A,
+                                              l1.data_ptr(), L, None, 0, s))
+        _lib.check(_lib.lib.rpyb_dyadic_query(h, 25, a.ctypes.data, b.ctypes.data, A,
+                                              None, 0, s1.data_ptr(), T + 3, s))
+        _lib.check(_lib.lib.rpyb_dyadic_query(h, 25, a.ctypes.data, b.ctypes.data, A,
+                                              l2.data_ptr(), L, s2.data_ptr(), T, s))
+        assert torch.equal(l1, l2)
+        assert torch.equal(s1[:, :T], s2)
+        emb = torch.zeros((25, T), dtype=torch.float64, device="cuda")
+        rpc._internals.dense_lie_to_tensor(emb, l1, rpc.LieBasis(w, d).get_l2t_matrix(),
+                                           rpc.LieBasis(w, d), rpc.TensorBasis(w, d))
+        ex = torch.zeros_like(emb)
+        rpc._internals.dense_ft_exp(ex, emb, rpc.TensorBasis(w, d))
+        assert float((ex - s2).abs().max()) <= 1e-13 * float(s2.abs().max())
+        bad_a, bad_b = np.array([0.5]), np.array([0.25])
+        rc = _lib.lib.rpyb_dyadic_query(h, 1, bad_a.ctypes.data, bad_b.ctypes.data, A,
+                                        l1.data_ptr(), L, None, 0, s)
+        assert rc == _lib.E_INVALID
+        rc = _lib.lib.rpyb_dyadic_query(h, 1, a.ctypes.data, b.ctypes.data, A, None, 0, None, 0, s)
+        assert rc == _lib.E_INVALID
+    finally:
+        _lib.lib.rpyb_dyadic_free(h)
+
+
+def test_c_abi_build_rejects_unsorted_times_and_bad_rows():
+    import ctypes
+    import torch
+    from roughpy_b200 import _lib
+    h = ctypes.c_void_p()
+    t = np.array([0.5, 0.25])
+    rows = torch.zeros((2, 3), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert _lib.lib.rpyb_dyadic_build(_lib.F64, 3, 3, 2, 0.0, 1.0, 2, t.ctypes.data,
+                                      rows.data_ptr(), 3, ctypes.byref(h), s) == _lib.E_INVALID
+    t = np.array([0.25, 0.5])
+    assert _lib.lib.rpyb_dyadic_build(_lib.F64, 3, 3, 2, 0.0, 1.0, 2, t.ctypes.data,
+                                      rows.data_ptr(), 4, ctypes.byref(h), s) == _lib.E_INVALID
+    assert not h.value
