@@ -14,8 +14,8 @@
  *    level k of a width-d tensor starts at degree_begin[k] = (d^k - 1)/(d - 1);
  *    inside a level, word (a_1 ... a_k) sits at sum_i a_i d^(k-i) (first letter
  *    most significant).  A batch is `batch` rows, row b at base + b*ld.
- *  - dtype: RPYB_F32 (float32 storage; products accumulated with compensated,
- *    double-float two-sum/two-product arithmetic) or RPYB_F64.
+ *  - dtype: RPYB_F32 (float32 storage; the exact products of float32 words
+ *    are accumulated in float64 and rounded once) or RPYB_F64.
  *  - Degree bounds follow roughpy.compute: a max_degree of -1 (or larger than
  *    depth) means `depth`.
  *  - Calls are asynchronous with respect to the host unless stated.  They are

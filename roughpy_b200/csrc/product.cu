@@ -71,8 +71,11 @@ struct Acc<float> {
     __device__ __forceinline__ float value() const { return df_value(v); }
 };
 
-// Alternative float32 accumulators (selected by RPYB_F32_ACC for measurement):
-// float64 accumulation of the exact float32 products, and plain float32 FMA.
+// float32 accumulators.  The default accumulates the exact float32 products
+// in float64 (one conversion and one FP64 FMA per product; 53 significant
+// bits, more than the double-float pair above, and faster on B200).
+// RPYB_F32_ACC selects the double-float pair ("df") or plain float32 FMAs
+// ("plain") for comparison.
 struct AccF32in64 {
     double v;
     __device__ __forceinline__ void init(float x) { v = (double)x; }
@@ -238,10 +241,10 @@ int f32_acc_mode()
 {
     static int m = [] {
         const char* e = getenv("RPYB_F32_ACC");
-        if (!e) return 0;
-        if (e[0] == 'f') return 1;   // "f64"
+        if (!e) return 1;            // float64 accumulation
+        if (e[0] == 'd') return 0;   // "df": double-float pair
         if (e[0] == 'p') return 2;   // "plain"
-        return 0;
+        return 1;
     }();
     return m;
 }
