@@ -360,6 +360,29 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* tree, int64_t n_queries,
                                int32_t resolution, double* out_logsig, int64_t ld_logsig,
                                double* out_sig, int64_t ld_sig, void* stream);
 
+/*
+ * Forward-mode derivative of signatures along Lie perturbations, batched over
+ * independent lists.  List q holds the pairs i in [offsets_host[q],
+ * offsets_host[q+1]) of rows of `logsig` (the log-signature of an interval)
+ * and `perturbation`, both Hall-basis Lie coordinates ([items, ld_lie] device
+ * arrays of dtype).  With X = l2t(logsig_i), P = l2t(perturbation_i):
+ *   out[q] = 0;  out[q] <- out[q] * exp(X) + exp(X) * sum_k (-1)^k ad_X^k(P) / (k+1)!
+ * over the list in order, exactly as the reference states it; for one pair
+ * this is the directional derivative of exp at X along P.  Scratch from
+ * `workspace` (rpyb_sig_derivative_workspace_size) or, when NULL, stream-
+ * ordered allocation.
+ * Replaces: algebra/src/lite_context.h:577-636 (LiteContext::sig_derivative_impl,
+ *           derive_series_compute, sig_derivative_single), reached from
+ *           Stream::signature_derivative (streams/src/stream.cpp:173-230).
+ */
+RPYB_API int64_t rpyb_sig_derivative_workspace_size(int dtype, int32_t width, int32_t depth,
+                                                    int64_t n_lists, int64_t n_items);
+RPYB_API int rpyb_sig_derivative(int dtype, int32_t width, int32_t depth, int64_t n_lists,
+                                 const int64_t* offsets_host, const void* logsig,
+                                 const void* perturbation, int64_t ld_lie, void* out,
+                                 int64_t ld_out, void* workspace, size_t workspace_bytes,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

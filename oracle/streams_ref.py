@@ -104,11 +104,11 @@ def stream_param_to_resolution(length):
 class Arith:
     """Dense float64 tensor arithmetic used by the restatement."""
 
-    def __init__(self, width, depth, l2t, t2l, exp, fmexp, log):
+    def __init__(self, width, depth, l2t, t2l, exp, fmexp, log, mul=None):
         self.width, self.depth = width, depth
         self.l2t = np.asarray(l2t, dtype=np.float64)   # [tensor, lie]
         self.t2l = np.asarray(t2l, dtype=np.float64)   # [lie, tensor]
-        self.exp, self.fmexp, self.log = exp, fmexp, log
+        self.exp, self.fmexp, self.log, self.mul = exp, fmexp, log, mul
         self.T = self.l2t.shape[0]
         self.L = self.l2t.shape[1]
 
@@ -118,7 +118,8 @@ class Arith:
         return cls(width, depth, l2t, t2l,
                    lambda x: oracle.ft_exp(width, depth, x),
                    lambda a, x: oracle.ft_fmexp(width, depth, a, x),
-                   lambda x: oracle.ft_log(width, depth, x))
+                   lambda x: oracle.ft_log(width, depth, x),
+                   lambda a, b: oracle.ft_mul(width, depth, a, b))
 
     def cbh(self, lies):
         # context.cpp:187-208
@@ -133,6 +134,25 @@ class Arith:
 
     def to_signature(self, lie):
         return self.exp(self.l2t @ lie)
+
+    def sig_derivative(self, pairs):
+        """algebra/src/lite_context.h:577-636 (sig_derivative_impl with
+        derive_series_compute and sig_derivative_single), for a list of
+        (log-signature, perturbation) Lie coordinate pairs."""
+        result = np.zeros(self.T)
+        for lie, pert in pairs:
+            x = self.l2t @ np.asarray(lie, dtype=np.float64)
+            p = self.l2t @ np.asarray(pert, dtype=np.float64)
+            sig = self.exp(x)
+            series = p.copy()
+            factor = 1.0
+            ad = self.mul(x, p) - self.mul(p, x)
+            for d in range(1, self.depth + 1):
+                factor *= d + 1
+                series = series + ad / factor if d % 2 == 0 else series - ad / factor
+                ad = self.mul(x, ad) - self.mul(ad, x)
+            result = self.mul(result, sig) + self.mul(sig, series)
+        return result
 
 
 class StreamRef:

@@ -46,7 +46,7 @@ from . import compute as rpc
 from . import signatures as S
 
 __all__ = ["RealInterval", "DyadicInterval", "to_dyadic_intervals", "LieIncrementStream",
-           "param_to_resolution"]
+           "param_to_resolution", "sig_derivative", "sig_derivative_batch"]
 
 
 class RealInterval:
@@ -311,11 +311,86 @@ class LieIncrementStream:
         lie = self._log_signature_batch(np.array([a]), np.array([b]), resolution)
         return self._truncate_lie(lie[0].cpu().numpy(), depth)
 
+    def signature_derivative(self, interval, perturbation=None, resolution=None, depth=None):
+        """Derivative of the signature along Lie perturbations
+        (streams/src/stream.cpp:173-230): ``interval`` with one
+        ``perturbation`` (Hall coordinates), or a list of (interval,
+        perturbation) pairs.  Each interval's log-signature comes from the
+        dyadic tree; float64 numpy tensor."""
+        if perturbation is None:
+            pairs = list(interval)
+        else:
+            pairs = [(interval, perturbation)]
+        ivs = [self._interval_args(iv, None) if isinstance(iv, (RealInterval, DyadicInterval))
+               else self._interval_args(*iv) for iv, _ in pairs]
+        a = np.array([v[0] for v in ivs])
+        b = np.array([v[1] for v in ivs])
+        lies = self._query(a, b, resolution)[0]
+        L = self.lie_basis.size()
+        pert = np.zeros((len(pairs), L))
+        for i, (_, p) in enumerate(pairs):
+            p = np.asarray(getattr(p, "data", p), dtype=np.float64).reshape(-1)
+            pert[i, :min(L, p.size)] = p[:L]
+        out = sig_derivative_batch(lies, pert, [0, len(pairs)], self.width, self.depth,
+                                   self.device)
+        return self._truncate_tensor(out[0].cpu().numpy(), depth)
+
     def signature(self, interval_or_inf=None, sup=None, resolution=None, depth=None):
         """Signature over an interval (streams/src/stream.cpp:156-171), float64 numpy."""
         a, b = self._interval_args(interval_or_inf, sup)
         sig = self._query(np.array([a]), np.array([b]), resolution, False, True)[1]
         return self._truncate_tensor(sig[0].cpu().numpy(), depth)
+
+
+def sig_derivative_batch(logsigs, perturbations, offsets, width: int, depth: int,
+                         device="cuda") -> torch.Tensor:
+    """Forward-mode signature derivatives of many lists at once
+    (``rpyb_sig_derivative``): list q is the pairs ``offsets[q]:offsets[q+1]``
+    of rows of ``logsigs`` and ``perturbations`` (Hall coordinates).  The
+    float64 or float32 dtype of ``logsigs`` is kept.  Returns ``[n_lists, T]``.
+    Replaces Context::sig_derivative (algebra/src/lite_context.h:577-636)."""
+    dev = torch.device(device)
+    lg = torch.as_tensor(np.asarray(logsigs) if not torch.is_tensor(logsigs) else logsigs)
+    dt = torch.float32 if lg.dtype == torch.float32 else torch.float64
+    lg = lg.to(dev, dt).contiguous()
+    pt = torch.as_tensor(np.asarray(perturbations) if not torch.is_tensor(perturbations)
+                         else perturbations).to(dev, dt).contiguous()
+    L = rpc.LieBasis(width, depth).size()
+    T = rpc.TensorBasis(width, depth).size()
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    n = off.shape[0] - 1
+    n_items = int(off[-1])
+    if lg.dim() != 2 or lg.shape != pt.shape or lg.shape[0] != n_items or lg.shape[1] != L:
+        raise ValueError("logsigs and perturbations must be [items, lie_dim] matching offsets")
+    code = _lib.F64 if dt == torch.float64 else _lib.F32
+    out = torch.empty((n, T), dtype=dt, device=dev)
+    ws_n = int(_lib.lib.rpyb_sig_derivative_workspace_size(code, width, depth, n, n_items))
+    if ws_n < 0:
+        raise ValueError(_lib.last_error())
+    ws = torch.empty(max(ws_n, 1), dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        _lib.check(_lib.lib.rpyb_sig_derivative(
+            code, width, depth, n, off.ctypes.data, lg.data_ptr() if n_items else None,
+            pt.data_ptr() if n_items else None, L, out.data_ptr(), T, ws.data_ptr(), ws.numel(),
+            torch.cuda.current_stream(dev).cuda_stream))
+    return out
+
+
+def sig_derivative(pairs, width: int, depth: int, device="cuda") -> np.ndarray:
+    """Derivative of the signature along the perturbations of one list of
+    (log-signature, perturbation) pairs, as Context::sig_derivative computes
+    it; float64 numpy result."""
+    pairs = list(pairs)
+    L = rpc.LieBasis(width, depth).size()
+    lg = np.zeros((len(pairs), L))
+    pt = np.zeros((len(pairs), L))
+    for i, (x, p) in enumerate(pairs):
+        x = np.asarray(x, dtype=np.float64).reshape(-1)
+        p = np.asarray(p, dtype=np.float64).reshape(-1)
+        lg[i, :min(L, x.size)] = x[:L]
+        pt[i, :min(L, p.size)] = p[:L]
+    out = sig_derivative_batch(lg, pt, [0, len(pairs)], width, depth, device)
+    return out[0].cpu().numpy()
 
 
 class _DyadicTree:

@@ -135,3 +135,30 @@ def test_shared_gradient_row_and_checkpoint_interval_invariance():
         grads.append(x.grad)
     for g in grads[1:]:
         assert float((g - grads[0]).abs().max()) <= 1e-12 * float(grads[0].abs().max())
+
+
+@pytest.mark.parametrize("w,d", [(3, 4), (5, 3), (2, 6)])
+def test_adjoint_matches_forward_mode_sig_derivative(w, d):
+    """<W, J v> from the forward-mode derivative (rpyb_sig_derivative, the
+    reference's sig_derivative) equals <J^T W, v> from the adjoint kernel,
+    for one-step streams (where the reference's recurrence is the Jacobian)."""
+    from roughpy_b200 import compute as rpc
+    from roughpy_b200.streams import sig_derivative_batch
+    rng = np.random.default_rng(w * 7 + d)
+    n = 6
+    L = rpc.LieBasis(w, d).size()
+    T = S.tensor_size(w, d)
+    x = rng.normal(0, 0.5, (n, w))
+    v = rng.normal(0, 1.0, (n, w))
+    W = torch.from_numpy(rng.normal(size=(n, T))).cuda()
+    lg = np.zeros((n, L))
+    pt = np.zeros((n, L))
+    lg[:, :w] = x
+    pt[:, :w] = v
+    jv = sig_derivative_batch(lg, pt, np.arange(n + 1), w, d)          # [n, T]
+    fwd = (W * jv).sum(dim=1)
+    plan = S.SignaturePlan(np.arange(n + 1), w, d, "f64")
+    xt = torch.from_numpy(x).cuda().requires_grad_(True)
+    (S.signature_with_grad(xt, plan) * W).sum().backward()
+    rev = (xt.grad * torch.from_numpy(v).cuda()).sum(dim=1)
+    assert float((fwd - rev).abs().max()) <= 1e-12 * max(1.0, float(fwd.abs().max()))

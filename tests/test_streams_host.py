@@ -111,3 +111,13 @@ def test_restated_stream_level_one_sums_and_linear_signature(golden):
     l2 = np.einsum("i,j->ij", inc, inc) / 2
     l3 = np.einsum("ij,k->ijk", l2, inc) / 3
     np.testing.assert_array_almost_equal(sig, np.hstack([[1.0], inc, l2.ravel(), l3.ravel()]))
+
+
+def test_restated_sig_derivative_known_answers(golden):
+    # tests/streams/test_lie_increment_path.py:233-263: one tick [0.2, 0.4, 0.6],
+    # perturbation e_2, interval [0, 1)
+    a = arith(golden, 3, 2)
+    got = a.sig_derivative([(np.array([0.2, 0.4, 0.6, 0.0, 0.0, 0.0]),
+                             np.array([0.0, 1.0, 0.0, 0.0, 0.0, 0.0]))])
+    want = np.array([0.0, 0.0, 1.0, 0.0, 0.0, 0.1, 0.0, 0.1, 0.4, 0.3, 0.0, 0.3, 0.0])
+    assert np.max(np.abs(got - want)) <= 1e-15
