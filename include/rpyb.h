@@ -361,6 +361,29 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* tree, int64_t n_queries,
                                double* out_sig, int64_t ld_sig, void* stream);
 
 /*
+ * Log-signatures / signatures of clopen intervals of a piecewise abelian
+ * stream: pieces j < n_pieces are [piece_inf[j], piece_sup[j]) (host arrays,
+ * in order) carrying Lie elements piece_lies ([n_pieces, ld_lies] device
+ * float64 Hall coordinates).  Each query is trimmed to [support_inf,
+ * support_sup), dissected at `resolution` (RPYB_QUERY_RESOLUTION_AUTO: the
+ * reference's per-query choice from default_resolution), and each dyadic
+ * interval [a, b) collects the pieces meeting it: whole when inside, else
+ * scaled by (sup_j - a) / (sup_j - inf_j) as the reference does; all
+ * contributions are combined by CBH (the log of the ordered product of their
+ * exponentials, in float64).  Outputs as rpyb_dyadic_query.
+ * Replaces: streams/src/piecewise_abelian_stream.cpp:154-189 through
+ *           streams/src/stream_base.cpp:81-96 and streams/src/stream.cpp:54-171.
+ */
+RPYB_API int rpyb_piecewise_query(int32_t width, int32_t depth, int64_t n_pieces,
+                                  const double* piece_inf, const double* piece_sup,
+                                  const double* piece_lies, int64_t ld_lies, double support_inf,
+                                  double support_sup, int32_t default_resolution,
+                                  int64_t n_queries, const double* inf_host,
+                                  const double* sup_host, int32_t resolution, double* out_logsig,
+                                  int64_t ld_logsig, double* out_sig, int64_t ld_sig,
+                                  void* stream);
+
+/*
  * Forward-mode derivative of signatures along Lie perturbations, batched over
  * independent lists.  List q holds the pairs i in [offsets_host[q],
  * offsets_host[q+1]) of rows of `logsig` (the log-signature of an interval)

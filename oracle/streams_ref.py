@@ -236,3 +236,41 @@ class StreamRef:
 
     def signature(self, inf=None, sup=None, resolution=None):
         return self.a.to_signature(self.log_signature(inf, sup, resolution))
+
+
+class PiecewiseRef:
+    """PiecewiseAbelianStream + Stream queries, restated
+    (streams/src/piecewise_abelian_stream.cpp:154-189 through
+    streams/src/stream_base.cpp:81-96 and streams/src/stream.cpp:37-171; the
+    Python constructor's support and resolution,
+    roughpy/src/streams/piecewise_abelian_stream.cpp:51-95)."""
+
+    def __init__(self, arith, pieces, resolution=None):
+        # pieces: [(inf, sup, lie coordinates)] in order
+        self.a = arith
+        self.pieces = [(float(p), float(q), np.asarray(v, dtype=np.float64)) for p, q, v in pieces]
+        self.support = (min(p for p, _, _ in self.pieces), max(q for _, q, _ in self.pieces))
+        self.resolution = 0 if resolution is None else int(resolution)
+
+    def _dyadic_logsig(self, k, p):
+        a, b = math.ldexp(k, -p), math.ldexp(k + 1, -p)
+        lies = []
+        for pa, pb, lie in self.pieces:
+            if pa >= b:
+                break
+            if pb <= a:
+                continue
+            if pa >= a and pb <= b:
+                lies.append(lie)
+            else:
+                # the reference's branch condition `pb <= pb` always holds, so
+                # every partial overlap takes to_multiplier_upper(piece, a)
+                lies.append(lie * ((pb - a) / (pb - pa)))
+        if not lies:
+            return np.zeros(self.a.L)
+        return self.a.cbh(lies)
+
+    log_signature = StreamRef.log_signature
+
+    def signature(self, inf=None, sup=None, resolution=None):
+        return self.a.to_signature(self.log_signature(inf, sup, resolution))

@@ -18,11 +18,11 @@
 // as batched product launches over all items at once ([items, T] rows); the
 // per-list recurrence is then one gathered product launch per list position.
 #include <algorithm>
-#include <mutex>
 #include <vector>
 
 #include "common.cuh"
 #include "product.cuh"
+#include "stream_ops.cuh"
 
 namespace rpyb {
 namespace {
@@ -178,48 +178,6 @@ int derivative(const Geometry& g, int64_t n_lists, const int64_t* off, const T* 
     return RPYB_OK;
 }
 
-// l2t maps (CSR, float64 values) uploaded once per (device, width, depth)
-// and kept for the life of the process
-struct MapEntry {
-    int device;
-    int32_t width, depth;
-    int64_t* ptr;
-    int64_t* idx;
-    double* val;
-};
-
-int l2t_map(const Geometry& g, const MapEntry** out)
-{
-    static std::mutex mu;
-    static std::vector<MapEntry> entries;
-    int dev = 0;
-    RPYB_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    for (const auto& e : entries)
-        if (e.device == dev && e.width == g.width && e.depth == g.depth) {
-            *out = &e;
-            return RPYB_OK;
-        }
-    const int64_t nnz = rpyb_lie_map_csr(g.width, g.depth, 0, nullptr, nullptr, nullptr);
-    if (nnz < 0) return (int)nnz;
-    std::vector<int64_t> hp(g.size() + 1), hi(std::max<int64_t>(nnz, 1));
-    std::vector<double> hv(std::max<int64_t>(nnz, 1));
-    const int64_t got = rpyb_lie_map_csr(g.width, g.depth, 0, hp.data(), hi.data(), hv.data());
-    if (got < 0) return (int)got;
-    MapEntry e{dev, g.width, g.depth, nullptr, nullptr, nullptr};
-    RPYB_CUDA(cudaMalloc(&e.ptr, hp.size() * 8));
-    RPYB_CUDA(cudaMalloc(&e.idx, hi.size() * 8));
-    RPYB_CUDA(cudaMalloc(&e.val, hv.size() * 8));
-    RPYB_CUDA(cudaMemcpy(e.ptr, hp.data(), hp.size() * 8, cudaMemcpyHostToDevice));
-    RPYB_CUDA(cudaMemcpy(e.idx, hi.data(), hi.size() * 8, cudaMemcpyHostToDevice));
-    RPYB_CUDA(cudaMemcpy(e.val, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice));
-    entries.reserve(64);
-    if (entries.size() == entries.capacity()) return fail(RPYB_E_UNSUPPORTED, "too many cached maps");
-    entries.push_back(e);
-    *out = &entries.back();
-    return RPYB_OK;
-}
-
 size_t bytes_for(int dtype, const Geometry& g, int64_t n_lists, int64_t n_items)
 {
     const int64_t es = dtype == RPYB_F64 ? 8 : 4;
@@ -278,11 +236,11 @@ RPYB_API int rpyb_sig_derivative(int dtype, int32_t width, int32_t depth, int64_
     if (!logsig || !perturbation) return fail(RPYB_E_INVALID, "null Lie arrays");
     if (ld_lie < lie_dim) return fail(RPYB_E_INVALID, "ld_lie smaller than the Lie dimension");
 
-    const MapEntry* map = nullptr;
-    if ((rc = l2t_map(g, &map))) return rc;
-    const int64_t* d_ptr[2] = {map->ptr, nullptr};
-    const int64_t* d_idx[2] = {map->idx, nullptr};
-    const double* d_val[2] = {map->val, nullptr};
+    const LieMapsDev* maps = nullptr;
+    if ((rc = lie_maps_device(g, &maps))) return rc;
+    const int64_t* d_ptr[2] = {maps->l2t_ptr, nullptr};
+    const int64_t* d_idx[2] = {maps->l2t_idx, nullptr};
+    const double* d_val[2] = {maps->l2t_val, nullptr};
 
     Scratch sc(workspace, workspace_bytes, s);
     void* ws = nullptr;

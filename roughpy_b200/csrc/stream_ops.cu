@@ -1,0 +1,289 @@
+// Shared stream building blocks (see stream_ops.cuh).
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "stream_ops.cuh"
+
+namespace rpyb {
+namespace {
+
+template <typename T>
+__global__ void unit_rows_kernel(T* __restrict__ out, int64_t ld, int64_t cols,
+                                 const int64_t* __restrict__ idx, int64_t n)
+{
+    const int64_t total = n * cols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / cols, c = e - i * cols;
+        const int64_t r = idx ? idx[i] : i;
+        out[r * ld + c] = (c == 0) ? T(1) : T(0);
+    }
+}
+
+// dst[idx[i]] <- src[i] for i < n (rows of `cols` values)
+template <typename T>
+__global__ void scatter_rows_kernel(T* __restrict__ dst, int64_t ld_dst, const T* __restrict__ src,
+                                    int64_t ld_src, int64_t cols, const int64_t* __restrict__ idx,
+                                    int64_t n)
+{
+    const int64_t total = n * cols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / cols, c = e - i * cols;
+        dst[idx[i] * ld_dst + c] = src[i * ld_src + c];
+    }
+}
+
+unsigned grid_for(int64_t total)
+{
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 16));
+}
+
+// streams/include/roughpy/streams/stream_base.h:74-83 (query_resolution)
+int32_t query_param_to_resolution(double length)
+{
+    int e = 0;
+    std::frexp(length, &e);
+    return -std::min(0, e - 1);
+}
+
+int upload_csr(const Geometry& g, int which, int64_t n_rows, const int64_t** ptr,
+               const int64_t** idx, const double** val)
+{
+    const int64_t nnz = rpyb_lie_map_csr(g.width, g.depth, which, nullptr, nullptr, nullptr);
+    if (nnz < 0) return (int)nnz;
+    std::vector<int64_t> hp(n_rows + 1), hi(std::max<int64_t>(nnz, 1));
+    std::vector<double> hv(std::max<int64_t>(nnz, 1));
+    const int64_t got = rpyb_lie_map_csr(g.width, g.depth, which, hp.data(), hi.data(), hv.data());
+    if (got < 0) return (int)got;
+    int64_t* dp = nullptr;
+    int64_t* di = nullptr;
+    double* dv = nullptr;
+    RPYB_CUDA(cudaMalloc(&dp, hp.size() * 8));
+    RPYB_CUDA(cudaMalloc(&di, hi.size() * 8));
+    RPYB_CUDA(cudaMalloc(&dv, hv.size() * 8));
+    RPYB_CUDA(cudaMemcpy(dp, hp.data(), hp.size() * 8, cudaMemcpyHostToDevice));
+    RPYB_CUDA(cudaMemcpy(di, hi.data(), hi.size() * 8, cudaMemcpyHostToDevice));
+    RPYB_CUDA(cudaMemcpy(dv, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice));
+    *ptr = dp;
+    *idx = di;
+    *val = dv;
+    return RPYB_OK;
+}
+
+}  // namespace
+
+int lie_maps_device(const Geometry& g, const LieMapsDev** out)
+{
+    static std::mutex mu;
+    static LieMapsDev entries[128];
+    static int n_entries = 0;
+    int dev = 0;
+    RPYB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    for (int i = 0; i < n_entries; ++i)
+        if (entries[i].device == dev && entries[i].width == g.width && entries[i].depth == g.depth) {
+            *out = &entries[i];
+            return RPYB_OK;
+        }
+    if (n_entries == 128) return fail(RPYB_E_UNSUPPORTED, "too many cached Lie maps");
+    const int64_t lie_dim = rpyb_lie_basis_size(g.width, g.depth);
+    if (lie_dim < 0) return (int)lie_dim;
+    LieMapsDev e;
+    e.device = dev;
+    e.width = g.width;
+    e.depth = g.depth;
+    e.lie_dim = lie_dim;
+    int rc;
+    if ((rc = upload_csr(g, 0, g.size(), &e.l2t_ptr, &e.l2t_idx, &e.l2t_val)) ||
+        (rc = upload_csr(g, 1, lie_dim, &e.t2l_ptr, &e.t2l_idx, &e.t2l_val)))
+        return rc;
+    entries[n_entries] = e;
+    *out = &entries[n_entries++];
+    return RPYB_OK;
+}
+
+int unit_rows(int mode, void* out, int64_t ld, int64_t cols, const int64_t* idx, int64_t n,
+              cudaStream_t s)
+{
+    if (n <= 0) return RPYB_OK;
+    if (mode == RPYB_F64)
+        unit_rows_kernel<double><<<grid_for(n * cols), 256, 0, s>>>(static_cast<double*>(out), ld,
+                                                                    cols, idx, n);
+    else
+        unit_rows_kernel<float><<<grid_for(n * cols), 256, 0, s>>>(static_cast<float*>(out), ld,
+                                                                   cols, idx, n);
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
+int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, void* acc,
+                     const void* src, const std::vector<int64_t>& off,
+                     const std::vector<int64_t>& src_rows, cudaStream_t s)
+{
+    const int64_t T = g.size();
+    int64_t maxc = 0;
+    for (int64_t q = 0; q < n; ++q) maxc = std::max(maxc, off[q + 1] - off[q]);
+    if (n == 0 || maxc == 0) return RPYB_OK;
+    const bool mixed = acc_mode == RPYB_F64 && src_mode == RPYB_F32;
+    if (!mixed && acc_mode != src_mode) return fail(RPYB_E_INVALID, "unsupported dtype pair");
+    const int64_t es = acc_mode == RPYB_F64 ? 8 : 4;
+    // index lists of every position, uploaded in one copy: position r uses
+    // packed[2 pos[r] .. 2 pos[r] + m) (accumulator rows) followed by m
+    // source rows
+    std::vector<int64_t> pos(maxc + 1, 0), packed;
+    packed.reserve(2 * (size_t)off[n]);
+    int64_t max_active = 0;
+    for (int64_t r = 0; r < maxc; ++r) {
+        pos[r] = (int64_t)packed.size() / 2;
+        const size_t mark = packed.size();
+        for (int64_t q = 0; q < n; ++q)
+            if (off[q + 1] - off[q] > r) packed.push_back(q);
+        const int64_t m = (int64_t)(packed.size() - mark);
+        for (int64_t q = 0; q < n; ++q)
+            if (off[q + 1] - off[q] > r) packed.push_back(src_rows[off[q] + r]);
+        max_active = std::max(max_active, m);
+    }
+    pos[maxc] = (int64_t)packed.size() / 2;
+    Scratch sc(nullptr, 0, s);
+    void* mem = nullptr;
+    const size_t idx_bytes = (packed.size() * 8 + 255) / 256 * 256;
+    int rc;
+    if ((rc = sc.get(idx_bytes + (size_t)(max_active * T * es), &mem))) return rc;
+    int64_t* d_idx = static_cast<int64_t*>(mem);
+    void* tmp = static_cast<char*>(mem) + idx_bytes;
+    // the pageable source is read before cudaMemcpyAsync returns
+    RPYB_CUDA(cudaMemcpyAsync(d_idx, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice, s));
+    for (int64_t r = 0; r < maxc; ++r) {
+        const int64_t m = pos[r + 1] - pos[r];
+        const int64_t* q_idx = d_idx + 2 * pos[r];
+        const int64_t* n_idx = q_idx + m;
+        if (mixed)
+            rc = rpyb_ft_mul_gather_mixed(g.width, g.depth, m, static_cast<double*>(tmp),
+                                          static_cast<const double*>(acc),
+                                          static_cast<const float*>(src), T, nullptr, q_idx,
+                                          n_idx, 0, s);
+        else
+            rc = rpyb_ft_mul_gather(acc_mode, g.width, g.depth, m, tmp, acc, src, T, nullptr,
+                                    q_idx, n_idx, 0, s);
+        if (rc) return rc;
+        if (acc_mode == RPYB_F64)
+            scatter_rows_kernel<double><<<grid_for(m * T), 256, 0, s>>>(
+                static_cast<double*>(acc), T, static_cast<const double*>(tmp), T, T, q_idx, m);
+        else
+            scatter_rows_kernel<float><<<grid_for(m * T), 256, 0, s>>>(
+                static_cast<float*>(acc), T, static_cast<const float*>(tmp), T, T, q_idx, m);
+        RPYB_CUDA(cudaGetLastError());
+    }
+    return RPYB_OK;
+}
+
+size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n)
+{
+    n = std::max<int64_t>(n, 1);
+    const int64_t log_ws = rpyb_ft_log_workspace_size(RPYB_F64, g.width, g.depth, n);
+    const int64_t exp_ws = rpyb_ft_exp_workspace_size(RPYB_F64, g.width, g.depth, n);
+    const size_t buf = (size_t)((n * g.size() * 8 + 255) / 256 * 256);
+    const size_t lbuf = (size_t)((n * lie_dim * 8 + 255) / 256 * 256);
+    return buf + lbuf + (size_t)std::max<int64_t>(std::max(log_ws, exp_ws), 1);
+}
+
+int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double* acc,
+                   double* out_logsig, int64_t ld_logsig, double* out_sig, int64_t ld_sig,
+                   void* scratch, size_t scratch_bytes, cudaStream_t s)
+{
+    if (m <= 0) return RPYB_OK;
+    const int64_t T = g.size(), L = maps.lie_dim;
+    const size_t buf = (size_t)((m * T * 8 + 255) / 256 * 256);
+    const size_t lbuf = (size_t)((m * L * 8 + 255) / 256 * 256);
+    if (scratch_bytes < buf + lbuf + 1) return fail(RPYB_E_INVALID, "query scratch too small");
+    double* tmp = static_cast<double*>(scratch);
+    double* lie_tmp = reinterpret_cast<double*>(static_cast<char*>(scratch) + buf);
+    void* ws = static_cast<char*>(scratch) + buf + lbuf;
+    const size_t wsb = scratch_bytes - buf - lbuf;
+    int rc;
+    // log in float64 (its incoming out[0] must be zero), then tensor -> Lie
+    RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
+    if ((rc = rpyb_ft_log(RPYB_F64, g.width, g.depth, m, tmp, acc, T, T, -1, -1, ws, wsb, s)))
+        return rc;
+    double* lie = out_logsig ? out_logsig : lie_tmp;
+    const int64_t ld_lie = out_logsig ? ld_logsig : L;
+    // the sparse map accumulates: clear its outputs first
+    RPYB_CUDA(cudaMemset2DAsync(lie, (size_t)(ld_lie * 8), 0, (size_t)(L * 8), (size_t)m, s));
+    if ((rc = rpyb_sparse_map(RPYB_F64, L, T, m, maps.t2l_ptr, maps.t2l_idx, maps.t2l_val, lie,
+                              tmp, ld_lie, T, 1.0, s)))
+        return rc;
+    if (out_sig) {
+        // algebra/src/context.cpp:156-159: exp(lie_to_tensor(log_signature))
+        RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
+        if ((rc = rpyb_sparse_map(RPYB_F64, T, L, m, maps.l2t_ptr, maps.l2t_idx, maps.l2t_val, tmp,
+                                  lie, T, ld_lie, 1.0, s)) ||
+            (rc = rpyb_ft_exp(RPYB_F64, g.width, g.depth, m, out_sig, tmp, ld_sig, T, -1, ws, wsb,
+                              s)))
+            return rc;
+    }
+    return RPYB_OK;
+}
+
+int refine_and_dissect(int64_t n, const double* inf, const double* sup, double s0, double s1,
+                       int32_t default_resolution, int32_t resolution, std::vector<int64_t>& k,
+                       std::vector<int32_t>& p, std::vector<int64_t>& poff)
+{
+    const bool auto_res = resolution == RPYB_QUERY_RESOLUTION_AUTO;
+    if (!auto_res && (resolution < -60 || resolution > 60))
+        return fail(RPYB_E_INVALID, "query resolution out of range");
+    std::vector<double> qi(n), qs(n);
+    std::vector<int32_t> tol(n);
+    std::vector<char> empty(n, 0);
+    int32_t max_tol = 0;
+    for (int64_t q = 0; q < n; ++q) {
+        double a = inf[q], b = sup[q];
+        if (!(a <= b)) return fail(RPYB_E_INVALID, "inf must not be larger than sup");
+        if (b < s0 || a > s1) {
+            empty[q] = 1;
+            a = b = s0;
+        } else {
+            a = std::max(a, s0);
+            b = std::min(b, s1);
+        }
+        if (b - a == 0.0) empty[q] = 1;
+        qi[q] = a;
+        qs[q] = b;
+        if (auto_res)
+            tol[q] = empty[q] ? default_resolution
+                              : std::max<int32_t>(default_resolution,
+                                                  query_param_to_resolution(b - a) + 2);
+        else
+            tol[q] = resolution;
+        max_tol = std::max(max_tol, std::abs(tol[q]));
+    }
+    const int64_t cap = std::max<int64_t>(1, n * (2 * (int64_t)max_tol + 130));
+    k.assign(cap, 0);
+    p.assign(cap, 0);
+    poff.assign(n + 1, 0);
+    int rc;
+    if ((rc = rpyb_dyadic_dissect_batch(n, qi.data(), qs.data(), tol.data(), 1, k.data(), p.data(),
+                                        cap, poff.data())))
+        return rc;
+    // empty queries keep no pieces
+    std::vector<int64_t> k2, off2(n + 1, 0);
+    std::vector<int32_t> p2;
+    k2.reserve(poff[n]);
+    p2.reserve(poff[n]);
+    for (int64_t q = 0; q < n; ++q) {
+        if (!empty[q])
+            for (int64_t i = poff[q]; i < poff[q + 1]; ++i) {
+                k2.push_back(k[i]);
+                p2.push_back(p[i]);
+            }
+        off2[q + 1] = (int64_t)k2.size();
+    }
+    k.swap(k2);
+    p.swap(p2);
+    poff.swap(off2);
+    return RPYB_OK;
+}
+
+}  // namespace rpyb

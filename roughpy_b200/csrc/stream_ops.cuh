@@ -1,0 +1,60 @@
+// Building blocks shared by the stream runtimes (dyadic tree, piecewise
+// abelian streams) and the signature derivative: Lie maps cached on the
+// device, ordered row products, and the log-signature / signature finish of
+// a batch of group-like products.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace rpyb {
+
+// CSR form of both Lie maps on the current device, uploaded once per
+// (device, width, depth) and kept for the life of the process.
+struct LieMapsDev {
+    int device = -1;
+    int32_t width = 0, depth = 0;
+    int64_t lie_dim = 0;
+    const int64_t* l2t_ptr = nullptr;   // tensor_size rows x lie_dim
+    const int64_t* l2t_idx = nullptr;
+    const double* l2t_val = nullptr;
+    const int64_t* t2l_ptr = nullptr;   // lie_dim rows x tensor_size
+    const int64_t* t2l_idx = nullptr;
+    const double* t2l_val = nullptr;
+};
+int lie_maps_device(const Geometry& g, const LieMapsDev** out);
+
+// rows idx[i] (or i) of `out` (stride ld) <- the unit tensor
+int unit_rows(int mode, void* out, int64_t ld, int64_t cols, const int64_t* idx, int64_t n,
+              cudaStream_t s);
+
+// acc[q] <- acc[q] * src[r_0] * src[r_1] * ... with q's source rows
+// src_rows[off[q] .. off[q+1]) in order; one gathered product per position.
+// acc_mode RPYB_F64 with src_mode RPYB_F32 uses the mixed-precision product.
+int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, void* acc,
+                     const void* src, const std::vector<int64_t>& off,
+                     const std::vector<int64_t>& src_rows, cudaStream_t s);
+
+// Bytes of scratch finish_queries needs for up to `n` rows.
+size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n);
+
+// For m group-like float64 rows `acc` ([m, T], overwritten): log-signature
+// t2l(log(acc)) into out_logsig and/or signature exp(l2t(logsig)) into
+// out_sig (either may be null).  Scratch from `scratch`.
+int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double* acc,
+                   double* out_logsig, int64_t ld_logsig, double* out_sig, int64_t ld_sig,
+                   void* scratch, size_t scratch_bytes, cudaStream_t s);
+
+// Stream::refine_interval (streams/src/stream.cpp:37-71) for a batch of
+// clopen queries against a support, then to_dyadic_intervals
+// (intervals/src/dyadic_interval.cpp:191-224).  resolution ==
+// RPYB_QUERY_RESOLUTION_AUTO picks max(default_resolution,
+// query_resolution(length) + 2) per query.  Empty (trimmed-away or zero
+// length) queries get no pieces.  Piece i of query q, in [poff[q],
+// poff[q+1]), is [k[i], k[i]+1) / 2^p[i].
+int refine_and_dissect(int64_t n, const double* inf, const double* sup, double s0, double s1,
+                       int32_t default_resolution, int32_t resolution, std::vector<int64_t>& k,
+                       std::vector<int32_t>& p, std::vector<int64_t>& poff);
+
+}  // namespace rpyb

@@ -46,7 +46,8 @@ from . import compute as rpc
 from . import signatures as S
 
 __all__ = ["RealInterval", "DyadicInterval", "to_dyadic_intervals", "LieIncrementStream",
-           "param_to_resolution", "sig_derivative", "sig_derivative_batch"]
+           "PiecewiseAbelianStream", "param_to_resolution", "sig_derivative",
+           "sig_derivative_batch"]
 
 
 class RealInterval:
@@ -126,7 +127,96 @@ def _dissect_batch(infs, sups, tols):
     return k[:m], p[:m], off
 
 
-class LieIncrementStream:
+class _StreamQueries:
+    """Query front end shared by the stream classes (the reference's
+    Stream::log_signature / signature / signature_derivative and its Python
+    argument rules, roughpy/src/streams/signature_arguments.cpp:56-160).
+    Subclasses provide ``_query(infs, sups, resolution, logsig, sig)``."""
+
+    def _interval_args(self, interval_or_inf, sup, resolution=None):
+        """(inf, sup, resolution): an interval, an inf/sup pair, nothing (the
+        whole support) or an integer alone (a resolution over the support)."""
+        if interval_or_inf is None:
+            return self.support.inf, self.support.sup, resolution
+        if isinstance(interval_or_inf, (RealInterval, DyadicInterval)):
+            return interval_or_inf.inf, interval_or_inf.sup, resolution
+        if sup is None:
+            if isinstance(interval_or_inf, (int, np.integer)) and not isinstance(interval_or_inf, bool):
+                return self.support.inf, self.support.sup, int(interval_or_inf)
+            raise TypeError("expecting integer resolution")
+        if float(interval_or_inf) > float(sup):
+            raise ValueError("inf must not be larger than sup")
+        return float(interval_or_inf), float(sup), resolution
+
+    def _truncate_lie(self, lie, depth):
+        if depth is None or depth >= self.depth:
+            return lie
+        return lie[..., :int(self.lie_basis.degree_begin[depth + 1]) - 1]
+
+    def _truncate_tensor(self, t, depth):
+        if depth is None or depth >= self.depth:
+            return t
+        return t[..., :int(self.tensor_basis.degree_begin[depth + 1])]
+
+    def log_signature_batch(self, infs, sups, resolution=None, chunk=16384):
+        """Log-signatures (Hall coordinates, float64) of many clopen intervals."""
+        infs = np.asarray(infs, dtype=np.float64).reshape(-1)
+        sups = np.asarray(sups, dtype=np.float64).reshape(-1)
+        outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution)[0]
+                for i in range(0, infs.shape[0], chunk)]
+        if not outs:
+            return torch.zeros((0, self.lie_basis.size()), dtype=torch.float64, device=self.device)
+        return torch.cat(outs)
+
+    def signature_batch(self, infs, sups, resolution=None, chunk=16384):
+        """Signatures exp(l2t(log_signature)) (float64) of many clopen intervals."""
+        infs = np.asarray(infs, dtype=np.float64).reshape(-1)
+        sups = np.asarray(sups, dtype=np.float64).reshape(-1)
+        outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution, False, True)[1]
+                for i in range(0, infs.shape[0], chunk)]
+        if not outs:
+            return torch.zeros((0, self.tensor_basis.size()), dtype=torch.float64,
+                               device=self.device)
+        return torch.cat(outs)
+
+    def _log_signature_batch(self, infs, sups, resolution=None):
+        return self._query(infs, sups, resolution)[0]
+
+    def log_signature(self, interval_or_inf=None, sup=None, resolution=None, depth=None):
+        """Log-signature over an interval (streams/src/stream.cpp:125-154), float64 numpy."""
+        a, b, res = self._interval_args(interval_or_inf, sup, resolution)
+        lie = self._query(np.array([a]), np.array([b]), res)[0]
+        return self._truncate_lie(lie[0].cpu().numpy(), depth)
+
+    def signature(self, interval_or_inf=None, sup=None, resolution=None, depth=None):
+        """Signature over an interval (streams/src/stream.cpp:156-171), float64 numpy."""
+        a, b, res = self._interval_args(interval_or_inf, sup, resolution)
+        sig = self._query(np.array([a]), np.array([b]), res, False, True)[1]
+        return self._truncate_tensor(sig[0].cpu().numpy(), depth)
+
+    def signature_derivative(self, interval, perturbation=None, resolution=None, depth=None):
+        """Derivative of the signature along Lie perturbations
+        (streams/src/stream.cpp:173-230): ``interval`` with one
+        ``perturbation`` (Hall coordinates), or a list of (interval,
+        perturbation) pairs.  Each interval's log-signature comes from the
+        stream's queries; float64 numpy tensor."""
+        pairs = list(interval) if perturbation is None else [(interval, perturbation)]
+        ivs = [self._interval_args(iv, None) if isinstance(iv, (RealInterval, DyadicInterval))
+               else self._interval_args(*iv) for iv, _ in pairs]
+        a = np.array([v[0] for v in ivs])
+        b = np.array([v[1] for v in ivs])
+        lies = self._query(a, b, resolution)[0]
+        L = self.lie_basis.size()
+        pert = np.zeros((len(pairs), L))
+        for i, (_, p) in enumerate(pairs):
+            p = np.asarray(getattr(p, "data", p), dtype=np.float64).reshape(-1)
+            pert[i, :min(L, p.size)] = p[:L]
+        out = sig_derivative_batch(lies, pert, [0, len(pairs)], self.width, self.depth,
+                                   self.device)
+        return self._truncate_tensor(out[0].cpu().numpy(), depth)
+
+
+class LieIncrementStream(_StreamQueries):
     """Stream of Lie increments with a GPU-resident dyadic signature tree."""
 
     def __init__(self, times, lies, width, depth, resolution, support, dtype=np.float64,
@@ -260,86 +350,75 @@ class LieIncrementStream:
                 stream))
         return lie, sg
 
-    def _log_signature_batch(self, infs, sups, resolution=None):
-        return self._query(infs, sups, resolution)[0]
 
-    def log_signature_batch(self, infs, sups, resolution=None, chunk=16384):
-        """Log-signatures (Hall coordinates, float64) of many clopen intervals."""
-        infs = np.asarray(infs, dtype=np.float64).reshape(-1)
-        sups = np.asarray(sups, dtype=np.float64).reshape(-1)
-        outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution)[0]
-                for i in range(0, infs.shape[0], chunk)]
-        if not outs:
-            return torch.zeros((0, self.lie_basis.size()), dtype=torch.float64, device=self.device)
-        return torch.cat(outs)
+class PiecewiseAbelianStream(_StreamQueries):
+    """A stream given as (interval, Lie element) pieces: RoughPy's
+    PiecewiseAbelianStream (streams/src/piecewise_abelian_stream.cpp), built
+    by ``construct`` as roughpy/src/streams/piecewise_abelian_stream.cpp:51-95
+    does (support = hull of the pieces, resolution 0 unless given).  Queries
+    run through ``rpyb_piecewise_query``."""
 
-    def signature_batch(self, infs, sups, resolution=None, chunk=16384):
-        """Signatures exp(l2t(log_signature)) (float64) of many clopen intervals."""
-        infs = np.asarray(infs, dtype=np.float64).reshape(-1)
-        sups = np.asarray(sups, dtype=np.float64).reshape(-1)
-        outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution, False, True)[1]
-                for i in range(0, infs.shape[0], chunk)]
-        if not outs:
-            return torch.zeros((0, self.tensor_basis.size()), dtype=torch.float64,
-                               device=self.device)
-        return torch.cat(outs)
+    def __init__(self, infs, sups, lies, width, depth, resolution, support, device="cuda"):
+        self.width, self.depth = int(width), int(depth)
+        self.resolution = int(resolution)
+        self.support = support
+        self.device = torch.device(device)
+        self.tensor_basis = rpc.TensorBasis(self.width, self.depth)
+        self.lie_basis = rpc.LieBasis(self.width, self.depth)
+        self.piece_inf = np.ascontiguousarray(infs, dtype=np.float64)
+        self.piece_sup = np.ascontiguousarray(sups, dtype=np.float64)
+        self.pieces = torch.from_numpy(np.ascontiguousarray(lies, dtype=np.float64)).to(self.device)
 
-    def _interval_args(self, interval_or_inf, sup):
-        if interval_or_inf is None:
-            return self.support.inf, self.support.sup
-        if isinstance(interval_or_inf, (RealInterval, DyadicInterval)):
-            return interval_or_inf.inf, interval_or_inf.sup
-        if sup is None:
-            raise TypeError("expected an interval or an inf, sup pair")
-        if float(interval_or_inf) > float(sup):
-            raise ValueError("inf must not be larger than sup")
-        return float(interval_or_inf), float(sup)
-
-    def _truncate_lie(self, lie, depth):
-        if depth is None or depth >= self.depth:
-            return lie
-        return lie[..., :int(self.lie_basis.degree_begin[depth + 1]) - 1]
-
-    def _truncate_tensor(self, t, depth):
-        if depth is None or depth >= self.depth:
-            return t
-        return t[..., :int(self.tensor_basis.degree_begin[depth + 1])]
-
-    def log_signature(self, interval_or_inf=None, sup=None, resolution=None, depth=None):
-        """Log-signature over an interval (streams/src/stream.cpp:125-154), float64 numpy."""
-        a, b = self._interval_args(interval_or_inf, sup)
-        lie = self._log_signature_batch(np.array([a]), np.array([b]), resolution)
-        return self._truncate_lie(lie[0].cpu().numpy(), depth)
-
-    def signature_derivative(self, interval, perturbation=None, resolution=None, depth=None):
-        """Derivative of the signature along Lie perturbations
-        (streams/src/stream.cpp:173-230): ``interval`` with one
-        ``perturbation`` (Hall coordinates), or a list of (interval,
-        perturbation) pairs.  Each interval's log-signature comes from the
-        dyadic tree; float64 numpy tensor."""
-        if perturbation is None:
-            pairs = list(interval)
+    @classmethod
+    def construct(cls, data, width=None, depth=None, resolution=None, dtype=None, ctx=None,
+                  device="cuda", **kwargs):
+        """``data``: (interval, Lie) pairs, the interval a RealInterval or an
+        (inf, sup) pair, the Lie element its Hall coordinates."""
+        if ctx is not None:
+            width = width or getattr(ctx, "width", None)
+            depth = depth or getattr(ctx, "depth", None)
+        if kwargs:
+            raise TypeError(f"unexpected keyword arguments {sorted(kwargs)}")
+        if not width or not depth:
+            raise ValueError("cannot deduce width/depth/ctype")
+        L = rpc.LieBasis(width, depth).size()
+        infs, sups, lies = [], [], []
+        for iv, lie in data:
+            a, b = (iv.inf, iv.sup) if isinstance(iv, (RealInterval, DyadicInterval)) else iv
+            infs.append(float(a))
+            sups.append(float(b))
+            v = np.asarray(getattr(lie, "data", lie), dtype=np.float64).reshape(-1)
+            row = np.zeros(L)
+            row[:min(L, v.size)] = v[:L]
+            lies.append(row)
+        if infs:
+            support = RealInterval(min(infs), max(sups))
         else:
-            pairs = [(interval, perturbation)]
-        ivs = [self._interval_args(iv, None) if isinstance(iv, (RealInterval, DyadicInterval))
-               else self._interval_args(*iv) for iv, _ in pairs]
-        a = np.array([v[0] for v in ivs])
-        b = np.array([v[1] for v in ivs])
-        lies = self._query(a, b, resolution)[0]
-        L = self.lie_basis.size()
-        pert = np.zeros((len(pairs), L))
-        for i, (_, p) in enumerate(pairs):
-            p = np.asarray(getattr(p, "data", p), dtype=np.float64).reshape(-1)
-            pert[i, :min(L, p.size)] = p[:L]
-        out = sig_derivative_batch(lies, pert, [0, len(pairs)], self.width, self.depth,
-                                   self.device)
-        return self._truncate_tensor(out[0].cpu().numpy(), depth)
+            support = RealInterval(0.0, 1.0)
+        lies = np.stack(lies) if lies else np.zeros((0, L))
+        return cls(infs, sups, lies, width, depth, 0 if resolution is None else resolution,
+                   support, device)
 
-    def signature(self, interval_or_inf=None, sup=None, resolution=None, depth=None):
-        """Signature over an interval (streams/src/stream.cpp:156-171), float64 numpy."""
-        a, b = self._interval_args(interval_or_inf, sup)
-        sig = self._query(np.array([a]), np.array([b]), resolution, False, True)[1]
-        return self._truncate_tensor(sig[0].cpu().numpy(), depth)
+    def _query(self, infs, sups, resolution, logsig=True, sig=False):
+        infs = np.ascontiguousarray(infs, dtype=np.float64).reshape(-1)
+        sups = np.ascontiguousarray(sups, dtype=np.float64).reshape(-1)
+        n = infs.shape[0]
+        L, T = self.lie_basis.size(), self.tensor_basis.size()
+        lie = torch.empty((n, L), dtype=torch.float64, device=self.device) if logsig else None
+        sg = torch.empty((n, T), dtype=torch.float64, device=self.device) if sig else None
+        if n == 0:
+            return lie, sg
+        res = _lib.QUERY_RESOLUTION_AUTO if resolution is None else int(resolution)
+        npc = int(self.piece_inf.shape[0])
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib.rpyb_piecewise_query(
+                self.width, self.depth, npc, self.piece_inf.ctypes.data if npc else None,
+                self.piece_sup.ctypes.data if npc else None,
+                self.pieces.data_ptr() if npc else None, L, float(self.support.inf),
+                float(self.support.sup), self.resolution, n, infs.ctypes.data, sups.ctypes.data,
+                res, lie.data_ptr() if logsig else None, L, sg.data_ptr() if sig else None, T,
+                torch.cuda.current_stream(self.device).cuda_stream))
+        return lie, sg
 
 
 def sig_derivative_batch(logsigs, perturbations, offsets, width: int, depth: int,

@@ -121,3 +121,18 @@ def test_restated_sig_derivative_known_answers(golden):
                              np.array([0.0, 1.0, 0.0, 0.0, 0.0, 0.0]))])
     want = np.array([0.0, 0.0, 1.0, 0.0, 0.0, 0.1, 0.0, 0.1, 0.4, 0.3, 0.0, 0.3, 0.0])
     assert np.max(np.abs(got - want)) <= 1e-15
+
+
+@pytest.mark.parametrize("count", [1, 2, 5])
+def test_restated_piecewise_full_data_is_cbh_of_the_pieces(golden, count):
+    # tests/streams/test_piecewise_lie_path.py:41-51: log_signature at
+    # resolution 5 over unit pieces [i, i+1) equals the CBH of all pieces
+    a = arith(golden, 4, 3)
+    rng = np.random.default_rng(count)
+    lies = []
+    for _ in range(count):
+        v = np.zeros(a.L)
+        v[:4] = rng.normal(0.0, 1.0, 4)
+        lies.append(v)
+    st = R.PiecewiseRef(a, [(float(i), float(i + 1), v) for i, v in enumerate(lies)])
+    np.testing.assert_array_almost_equal(st.log_signature(resolution=5), a.cbh(lies), decimal=12)
