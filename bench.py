@@ -45,10 +45,11 @@ SWEEP_BATCH = 1024
 E2E_CHUNKS = 8
 SM_COUNT_B200 = 148
 FP32_LANES_PER_SM = 128
-# dram bytes per launch of the float32 signature kernel on this workload,
-# from the ncu capture summarised in profiles/signature_f32c_w8d5.md
-# (captured on a 512-stream slice; DRAM traffic scales with the stream count).
-SIG_TRAFFIC_BYTES_PER_STREAM = None
+# DRAM bytes (read + write) per stream of the float32 signature kernel on this
+# workload: 68.1 + 97.4 MB measured by ncu on the 1024-stream slice
+# (`bench.py --profile-slice 1024`, profiles/signature_w8d5_f32c_f64.md); the
+# traffic is inputs plus outputs, so it scales with the number of streams.
+SIG_TRAFFIC_BYTES_PER_STREAM = (68.1e6 + 97.4e6) / 1024
 
 
 def log(*a):
@@ -261,8 +262,7 @@ def run_b200(args, rank, world, local_rank):
         sm_mhz = (clk or {}).get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
         fp32_peak = 2 * FP32_LANES_PER_SM * SM_COUNT_B200 * sm_mhz * 1e6 / 1e12
         algo_flops = 2.0 * FMA_PER_STEP * float(lens.sum())
-        achieved = algo_flops / (ms_step / 1e3) / 1e12 / world * world  # per GPU
-        achieved = algo_flops / (ms_step / 1e3) / 1e12
+        achieved = algo_flops / (ms_step / 1e3) / 1e12   # this GPU's launch
         traffic = (SIG_TRAFFIC_BYTES_PER_STREAM * N_STREAMS
                    if SIG_TRAFFIC_BYTES_PER_STREAM else None)
         sweep = fma_sweep(dev, pk["hbm_gbs"]) if not args.no_sweep else None
@@ -295,6 +295,8 @@ def run_b200(args, rank, world, local_rank):
                 "bound": "fp32_fma", "achieved": round(achieved, 3), "peak": round(fp32_peak, 2),
                 "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4),
                 "traffic": traffic,
+                "traffic_unit": "bytes per launch (ncu dram read+write, 1024-stream "
+                                "capture scaled by the stream count)",
                 "note": "algorithmic 2*42792 flop per increment; FP32 CUDA-core peak "
                         "= 148 SM x 128 lanes x 2 x sampled SM clock (no tensor cores on "
                         "this path)",
@@ -432,6 +434,12 @@ def dyadic_queries(dev):
     lies = {}
     for mode, data in (("f32c", inc.astype(np.float32)),
                        ("f64", inc.astype(np.float32).astype(np.float64))):
+        # warm-up on a small stream of the same shape: first-use costs (kernel
+        # module loading, Lie map upload, scratch pool growth) stay untimed
+        warm = LieIncrementStream.from_increments(data[:256], indices=idx[:256], width=6,
+                                                  depth=5, resolution=16, device=dev)
+        warm.log_signature_batch(q[:1000, 0] / 256, q[:1000, 1] / 256)
+        del warm
         st = LieIncrementStream.from_increments(data, indices=idx, width=6, depth=5,
                                                 resolution=16, device=dev)
         torch.cuda.synchronize()
@@ -439,7 +447,7 @@ def dyadic_queries(dev):
         st._build_tree()
         torch.cuda.synchronize()
         tb = time.perf_counter() - t0
-        st.log_signature_batch(q[:1000, 0], q[:1000, 1])
+        st.log_signature_batch(q[:, 0], q[:, 1])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         lie = st.log_signature_batch(q[:, 0], q[:, 1])

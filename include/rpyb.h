@@ -57,6 +57,14 @@ extern "C" {
 RPYB_API const char* rpyb_last_error(void);
 /* Library version string. */
 RPYB_API const char* rpyb_version(void);
+/*
+ * Entry points given no workspace take stream-ordered scratch from a
+ * library-owned memory pool per device, which keeps freed memory for reuse
+ * (repeated calls then map no device memory).  This returns the pooled
+ * memory of every device to the driver.  No reference counterpart.
+ */
+RPYB_API int rpyb_release_cached_memory(void);
+
 /* Number of scalars in a width/depth tensor: (width^(depth+1)-1)/(width-1). */
 RPYB_API int64_t rpyb_tensor_size(int32_t width, int32_t depth);
 

@@ -44,6 +44,7 @@ _pdbl = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "rpyb_last_error": (ctypes.c_char_p, []),
     "rpyb_version": (ctypes.c_char_p, []),
+    "rpyb_release_cached_memory": (_int, []),
     "rpyb_tensor_size": (_i64, [_i32, _i32]),
     "rpyb_ft_fma": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _pi32, _vp]),
     "rpyb_ft_mul_gather": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,

@@ -46,7 +46,8 @@ inline int32_t clamp_max_degree(int32_t d, int32_t depth)
 }
 
 // Stream-ordered scratch: uses the caller's workspace when given, otherwise
-// takes memory with cudaMallocAsync and releases it with cudaFreeAsync.
+// takes memory from the library's per-device pool (cudaMallocFromPoolAsync)
+// and releases it with cudaFreeAsync; the pool keeps freed memory for reuse.
 class Scratch {
 public:
     Scratch(void* ws, size_t ws_bytes, cudaStream_t s) : ws_(ws), cap_(ws_bytes), s_(s) {}

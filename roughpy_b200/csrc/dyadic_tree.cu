@@ -302,40 +302,12 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* t, int64_t n_queries,
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int R = t->resolution;
 
-    std::vector<int64_t> k, poff;
-    std::vector<int32_t> p;
-    if ((rc = refine_and_dissect(n_queries, inf_host, sup_host, t->s0, t->s1, R, resolution, k, p,
-                                 poff)))
-        return rc;
-
-    // pieces -> node rows (dyadic_caching_layer.cpp:86-130): at the stream
-    // resolution a leaf; coarser pieces are whole nodes; a finer piece maps
-    // to the leaf it starts in when the start points coincide, and is
-    // dropped otherwise.  Zero pieces are dropped.
-    std::vector<int64_t> qoff(n_queries + 1, 0), nodes;
-    nodes.reserve((size_t)poff[n_queries]);
-    for (int64_t q = 0; q < n_queries; ++q) {
-        for (int64_t i = poff[q]; i < poff[q + 1]; ++i) {
-            int64_t row;
-            if (p[i] <= R) {
-                row = node_row(t, (int64_t)R - p[i], k[i]);
-            } else {
-                const int sh = p[i] - R;
-                if (sh > 62) {
-                    row = (k[i] == 0) ? node_row(t, 0, 0) : -1;
-                } else {
-                    const int64_t tk = k[i] >> sh;   // floor division
-                    row = ((tk << sh) == k[i]) ? node_row(t, 0, tk) : -1;
-                }
-            }
-            if (row >= 0) nodes.push_back(row);
-        }
-        qoff[q + 1] = (int64_t)nodes.size();
-    }
-
-    // device, in chunks of queries bounded by a memory budget
+    // device buffers for chunks of queries bounded by a memory budget; the
+    // host work of a chunk (trim, dissection, node lookup) overlaps the
+    // device work of the previous one
     const int64_t budget = (int64_t)1 << 30;   // bytes per [chunk, T] float64 buffer
-    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_queries, budget / (T * 8)));
+    const int64_t chunk = std::max<int64_t>(
+        1, std::min<int64_t>({n_queries, budget / (T * 8), (int64_t)8192}));
     const size_t buf = (size_t)((chunk * T * 8 + 255) / 256 * 256);
     const size_t fin = finish_scratch_bytes(g, L, chunk);
     Scratch sc(nullptr, 0, s);
@@ -343,16 +315,43 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* t, int64_t n_queries,
     if ((rc = sc.get(buf + fin, &mem))) return rc;
     double* acc = static_cast<double*>(mem);
     void* fin_mem = static_cast<char*>(mem) + buf;
+    std::vector<int64_t> k, poff, qoff, nodes;
+    std::vector<int32_t> p;
     for (int64_t q0 = 0; q0 < n_queries; q0 += chunk) {
         const int64_t m = std::min(chunk, n_queries - q0);
-        std::vector<int64_t> loff(m + 1);
-        for (int64_t i = 0; i <= m; ++i) loff[i] = qoff[q0 + i] - qoff[q0];
-        std::vector<int64_t> rows_q(nodes.begin() + qoff[q0], nodes.begin() + qoff[q0 + m]);
+        if ((rc = refine_and_dissect(m, inf_host + q0, sup_host + q0, t->s0, t->s1, R, resolution,
+                                     k, p, poff)))
+            return rc;
+        // pieces -> node rows (dyadic_caching_layer.cpp:86-130): at the
+        // stream resolution a leaf; coarser pieces are whole nodes; a finer
+        // piece maps to the leaf it starts in when the start points
+        // coincide, and is dropped otherwise.  Zero pieces are dropped.
+        qoff.assign(m + 1, 0);
+        nodes.clear();
+        for (int64_t q = 0; q < m; ++q) {
+            for (int64_t i = poff[q]; i < poff[q + 1]; ++i) {
+                int64_t row;
+                if (p[i] <= R) {
+                    row = node_row(t, (int64_t)R - p[i], k[i]);
+                } else {
+                    const int sh = p[i] - R;
+                    if (sh > 62) {
+                        row = (k[i] == 0) ? node_row(t, 0, 0) : -1;
+                    } else {
+                        const int64_t tk = k[i] >> sh;   // floor division
+                        row = ((tk << sh) == k[i]) ? node_row(t, 0, tk) : -1;
+                    }
+                }
+                if (row >= 0) nodes.push_back(row);
+            }
+            qoff[q + 1] = (int64_t)nodes.size();
+        }
         if ((rc = unit_rows(RPYB_F64, acc, T, T, nullptr, m, s)) ||
-            (rc = ordered_products(RPYB_F64, t->mode, g, m, acc, t->nodes, loff, rows_q, s)) ||
-            (rc = finish_queries(g, *t->maps, m, acc, out_logsig ? out_logsig + q0 * ld_logsig : nullptr,
-                                 ld_logsig, out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig,
-                                 fin_mem, fin, s)))
+            (rc = ordered_products(RPYB_F64, t->mode, g, m, acc, t->nodes, qoff, nodes, s)) ||
+            (rc = finish_queries(g, *t->maps, m, acc,
+                                 out_logsig ? out_logsig + q0 * ld_logsig : nullptr, ld_logsig,
+                                 out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig, fin_mem, fin,
+                                 s)))
             return rc;
     }
     return RPYB_OK;

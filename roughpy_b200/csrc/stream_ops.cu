@@ -22,17 +22,19 @@ __global__ void unit_rows_kernel(T* __restrict__ out, int64_t ld, int64_t cols,
     }
 }
 
-// dst[idx[i]] <- src[i] for i < n (rows of `cols` values)
+// acc[order[i]] <- (parity[i] ? b1 : b0)[i] for i < n (rows of `cols` values)
 template <typename T>
-__global__ void scatter_rows_kernel(T* __restrict__ dst, int64_t ld_dst, const T* __restrict__ src,
-                                    int64_t ld_src, int64_t cols, const int64_t* __restrict__ idx,
-                                    int64_t n)
+__global__ void gather_final_kernel(T* __restrict__ acc, const T* __restrict__ b0,
+                                    const T* __restrict__ b1, int64_t cols,
+                                    const int64_t* __restrict__ order,
+                                    const int64_t* __restrict__ parity, int64_t n)
 {
     const int64_t total = n * cols;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = e / cols, c = e - i * cols;
-        dst[idx[i] * ld_dst + c] = src[i * ld_src + c];
+        const T* src = parity[i] ? b1 : b0;
+        acc[order[i] * cols + c] = src[i * cols + c];
     }
 }
 
@@ -124,59 +126,74 @@ int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, v
                      const std::vector<int64_t>& src_rows, cudaStream_t s)
 {
     const int64_t T = g.size();
-    int64_t maxc = 0;
-    for (int64_t q = 0; q < n; ++q) maxc = std::max(maxc, off[q + 1] - off[q]);
-    if (n == 0 || maxc == 0) return RPYB_OK;
+    if (n == 0) return RPYB_OK;
     const bool mixed = acc_mode == RPYB_F64 && src_mode == RPYB_F32;
     if (!mixed && acc_mode != src_mode) return fail(RPYB_E_INVALID, "unsupported dtype pair");
-    const int64_t es = acc_mode == RPYB_F64 ? 8 : 4;
-    // index lists of every position, uploaded in one copy: position r uses
-    // packed[2 pos[r] .. 2 pos[r] + m) (accumulator rows) followed by m
-    // source rows
-    std::vector<int64_t> pos(maxc + 1, 0), packed;
-    packed.reserve(2 * (size_t)off[n]);
-    int64_t max_active = 0;
+    // Rows sorted by factor count, most first: the rows still active at
+    // position r are then a prefix of the order, and the products ping-pong
+    // between two contiguous buffers without per-position scatters.
+    std::vector<int64_t> order;
+    order.reserve(n);
+    for (int64_t q = 0; q < n; ++q)
+        if (off[q + 1] > off[q]) order.push_back(q);
+    const int64_t n1 = (int64_t)order.size();
+    if (n1 == 0) return RPYB_OK;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+        return off[x + 1] - off[x] > off[y + 1] - off[y];
+    });
+    const int64_t maxc = off[order[0] + 1] - off[order[0]];
+    // host index block: order (n1), final parity (n1), then per position r
+    // the source rows of the m_r active rows
+    std::vector<int64_t> packed(order);
+    packed.reserve(2 * n1 + (size_t)off[n]);
+    for (int64_t i = 0; i < n1; ++i) packed.push_back((off[order[i] + 1] - off[order[i]] - 1) & 1);
+    std::vector<int64_t> pos(maxc + 1), active(maxc);
     for (int64_t r = 0; r < maxc; ++r) {
-        pos[r] = (int64_t)packed.size() / 2;
-        const size_t mark = packed.size();
-        for (int64_t q = 0; q < n; ++q)
-            if (off[q + 1] - off[q] > r) packed.push_back(q);
-        const int64_t m = (int64_t)(packed.size() - mark);
-        for (int64_t q = 0; q < n; ++q)
-            if (off[q + 1] - off[q] > r) packed.push_back(src_rows[off[q] + r]);
-        max_active = std::max(max_active, m);
+        pos[r] = (int64_t)packed.size();
+        int64_t m = 0;
+        while (m < n1 && off[order[m] + 1] - off[order[m]] > r) {
+            packed.push_back(src_rows[off[order[m]] + r]);
+            ++m;
+        }
+        active[r] = m;
     }
-    pos[maxc] = (int64_t)packed.size() / 2;
+    const int64_t es = acc_mode == RPYB_F64 ? 8 : 4;
+    const size_t idx_bytes = (packed.size() * 8 + 255) / 256 * 256;
+    const size_t buf = (size_t)((n1 * T * es + 255) / 256 * 256);
     Scratch sc(nullptr, 0, s);
     void* mem = nullptr;
-    const size_t idx_bytes = (packed.size() * 8 + 255) / 256 * 256;
     int rc;
-    if ((rc = sc.get(idx_bytes + (size_t)(max_active * T * es), &mem))) return rc;
+    if ((rc = sc.get(idx_bytes + 2 * buf, &mem))) return rc;
     int64_t* d_idx = static_cast<int64_t*>(mem);
-    void* tmp = static_cast<char*>(mem) + idx_bytes;
+    char* bufs[2] = {static_cast<char*>(mem) + idx_bytes, static_cast<char*>(mem) + idx_bytes + buf};
     // the pageable source is read before cudaMemcpyAsync returns
     RPYB_CUDA(cudaMemcpyAsync(d_idx, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice, s));
     for (int64_t r = 0; r < maxc; ++r) {
-        const int64_t m = pos[r + 1] - pos[r];
-        const int64_t* q_idx = d_idx + 2 * pos[r];
-        const int64_t* n_idx = q_idx + m;
+        const int64_t m = active[r];
+        const void* lhs = (r == 0) ? acc : bufs[(r - 1) & 1];
+        const int64_t* lhs_idx = (r == 0) ? d_idx : nullptr;   // gather by order at the start
+        void* out = bufs[r & 1];
+        const int64_t* rhs_idx = d_idx + pos[r];
         if (mixed)
-            rc = rpyb_ft_mul_gather_mixed(g.width, g.depth, m, static_cast<double*>(tmp),
-                                          static_cast<const double*>(acc),
-                                          static_cast<const float*>(src), T, nullptr, q_idx,
-                                          n_idx, 0, s);
+            rc = rpyb_ft_mul_gather_mixed(g.width, g.depth, m, static_cast<double*>(out),
+                                          static_cast<const double*>(lhs),
+                                          static_cast<const float*>(src), T, nullptr, lhs_idx,
+                                          rhs_idx, 0, s);
         else
-            rc = rpyb_ft_mul_gather(acc_mode, g.width, g.depth, m, tmp, acc, src, T, nullptr,
-                                    q_idx, n_idx, 0, s);
+            rc = rpyb_ft_mul_gather(acc_mode, g.width, g.depth, m, out, lhs, src, T, nullptr,
+                                    lhs_idx, rhs_idx, 0, s);
         if (rc) return rc;
-        if (acc_mode == RPYB_F64)
-            scatter_rows_kernel<double><<<grid_for(m * T), 256, 0, s>>>(
-                static_cast<double*>(acc), T, static_cast<const double*>(tmp), T, T, q_idx, m);
-        else
-            scatter_rows_kernel<float><<<grid_for(m * T), 256, 0, s>>>(
-                static_cast<float*>(acc), T, static_cast<const float*>(tmp), T, T, q_idx, m);
-        RPYB_CUDA(cudaGetLastError());
     }
+    // rows back to their places: row i of the order ends in buffer parity[i]
+    if (acc_mode == RPYB_F64)
+        gather_final_kernel<double><<<grid_for(n1 * T), 256, 0, s>>>(
+            static_cast<double*>(acc), reinterpret_cast<const double*>(bufs[0]),
+            reinterpret_cast<const double*>(bufs[1]), T, d_idx, d_idx + n1, n1);
+    else
+        gather_final_kernel<float><<<grid_for(n1 * T), 256, 0, s>>>(
+            static_cast<float*>(acc), reinterpret_cast<const float*>(bufs[0]),
+            reinterpret_cast<const float*>(bufs[1]), T, d_idx, d_idx + n1, n1);
+    RPYB_CUDA(cudaGetLastError());
     return RPYB_OK;
 }
 

@@ -30,8 +30,10 @@ int unit_rows(int mode, void* out, int64_t ld, int64_t cols, const int64_t* idx,
               cudaStream_t s);
 
 // acc[q] <- acc[q] * src[r_0] * src[r_1] * ... with q's source rows
-// src_rows[off[q] .. off[q+1]) in order; one gathered product per position.
-// acc_mode RPYB_F64 with src_mode RPYB_F32 uses the mixed-precision product.
+// src_rows[off[q] .. off[q+1]) in order; one gathered product per position,
+// ping-ponging between two scratch buffers in factor-count order, and one
+// gather back into acc (rows of stride T).  acc_mode RPYB_F64 with src_mode
+// RPYB_F32 uses the mixed-precision product.
 int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, void* acc,
                      const void* src, const std::vector<int64_t>& off,
                      const std::vector<int64_t>& src_rows, cudaStream_t s);

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -55,6 +57,36 @@ int make_geometry(int32_t width, int32_t depth, Geometry& g)
     return RPYB_OK;
 }
 
+// Library-owned stream-ordered memory pool per device.  Freed scratch stays
+// in the pool (release threshold: unlimited) so that repeated calls with
+// gigabyte temporaries do not map and unmap device memory each time;
+// rpyb_release_cached_memory returns it to the driver.
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+static int scratch_pool(cudaMemPool_t* out)
+{
+    int dev = 0;
+    RPYB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(RPYB_E_UNSUPPORTED, "device ordinal too large");
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        RPYB_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t threshold = UINT64_MAX;
+        RPYB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+        g_pools[dev] = pool;
+    }
+    *out = g_pools[dev];
+    return RPYB_OK;
+}
+
 Scratch::~Scratch()
 {
     if (owned_) cudaFreeAsync(owned_, s_);
@@ -73,7 +105,10 @@ int Scratch::get(size_t bytes, void** p)
         *p = ws_;
         return RPYB_OK;
     }
-    RPYB_CUDA(cudaMallocAsync(&owned_, bytes, s_));
+    cudaMemPool_t pool = nullptr;
+    int rc;
+    if ((rc = scratch_pool(&pool))) return rc;
+    RPYB_CUDA(cudaMallocFromPoolAsync(&owned_, bytes, pool, s_));
     *p = owned_;
     return RPYB_OK;
 }
@@ -117,6 +152,14 @@ static int horner_buffers(int dtype, const Geometry& g, int64_t batch, int nbuf,
 using namespace rpyb;
 
 extern "C" {
+
+RPYB_API int rpyb_release_cached_memory(void)
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (int d = 0; d < 64; ++d)
+        if (g_pools[d]) RPYB_CUDA(cudaMemPoolTrimTo(g_pools[d], 0));
+    return RPYB_OK;
+}
 
 RPYB_API const char* rpyb_last_error(void) { return rpyb::g_last_error.c_str(); }
 

@@ -229,7 +229,9 @@ class LieIncrementStream(_StreamQueries):
         self.mode = mode or ("f64" if self.dtype == np.float64 else "f32c")
         self.device = torch.device(device)
         self.times = np.asarray(times, dtype=np.float64)
-        self.lies = np.asarray(lies, dtype=np.float64)        # [n_events, lie_dim]
+        # [n_events, c] Hall coordinates of the events, c <= lie_dim (omitted
+        # trailing coordinates are zero)
+        self.lies = np.asarray(lies, dtype=np.float64)
         self.tensor_basis = rpc.TensorBasis(self.width, self.depth)
         self.lie_basis = rpc.LieBasis(self.width, self.depth)
         self._tree = None
@@ -264,8 +266,8 @@ class LieIncrementStream(_StreamQueries):
         if not width or not depth:
             raise ValueError("either ctx or both width and depth must be specified")
         lie_dim = rpc.LieBasis(width, depth).size()
-        lies = np.zeros((rows.shape[0], lie_dim), dtype=np.float64)
         ncol = min(rows.shape[1], lie_dim)
+        lies = np.zeros((rows.shape[0], max(ncol, width)), dtype=np.float64)
         lies[:, :ncol] = rows[:, :ncol]
         n = rows.shape[0]
         if indices is None:
@@ -315,7 +317,10 @@ class LieIncrementStream(_StreamQueries):
         if higher.size == 0 or not np.any(higher):
             rows, row_len = self.lies[:, :self.width], self.width
         else:
-            rows, row_len = self.lies, self.lies.shape[1]
+            L = self.lie_basis.size()
+            rows = np.zeros((self.lies.shape[0], L))
+            rows[:, :self.lies.shape[1]] = self.lies
+            row_len = L
         n = int(self.times.shape[0])
         rows_t = torch.from_numpy(np.ascontiguousarray(rows)).to(self.device, dt).contiguous()
         times = np.ascontiguousarray(self.times, dtype=np.float64)
