@@ -42,7 +42,7 @@ LEN_LO, LEN_HI = 16, 4096
 FMA_PER_STEP = 42792          # Horner Chen step at (8,5): sum_k sum_{i<=k} 8^i
 SWEEP = [(2, 12), (4, 8), (6, 6), (8, 6)]
 SWEEP_BATCH = 1024
-E2E_CHUNKS = 8
+E2E_CHUNKS = 16
 SM_COUNT_B200 = 148
 FP32_LANES_PER_SM = 128
 # DRAM bytes (read + write) per stream of the float32 signature kernel on this

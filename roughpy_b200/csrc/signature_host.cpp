@@ -2,8 +2,9 @@
 // the device, the signatures computed and copied back in chunks of streams,
 // with the host->device copy of chunk i+1 and the device->host copy of chunk
 // i-1 overlapping the kernel of chunk i (two copy streams, double-buffered
-// device chunks).  With pinned host buffers the PCIe transfers hide behind
-// the computation.
+// device chunks).  Consecutive kernels alternate between two compute streams
+// so that one chunk's kernel fills the tail of the previous one.  With pinned
+// host buffers the PCIe transfers hide behind the computation.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,6 +19,7 @@ namespace {
 
 struct CopyStreams {
     cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaStream_t comp = nullptr;   // second compute stream (odd chunks)
 };
 
 std::mutex g_cs_mu;
@@ -33,6 +35,7 @@ int copy_streams(CopyStreams** out)
     if (!c.h2d) {
         RPYB_CUDA(cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking));
         RPYB_CUDA(cudaStreamCreateWithFlags(&c.d2h, cudaStreamNonBlocking));
+        RPYB_CUDA(cudaStreamCreateWithFlags(&c.comp, cudaStreamNonBlocking));
     }
     *out = &c;
     return RPYB_OK;
@@ -43,13 +46,18 @@ struct Chunk {
     int64_t r0, r1;       // increment rows [r0, r1)
 };
 
+// Contiguous chunks of about equal total length, except that the first and
+// the last carry half a share: the first kernel starts after a shorter
+// upload and the last copy-out, which nothing overlaps, is shorter.
 std::vector<Chunk> split(const int64_t* off, int64_t n, int chunks)
 {
     std::vector<Chunk> out;
     const int64_t total = off[n];
+    const double shares = chunks > 2 ? chunks - 1.0 : (double)chunks;
     int64_t s = 0;
     for (int c = 0; c < chunks && s < n; ++c) {
-        const int64_t target = (c + 1 == chunks) ? total : total * (c + 1) / chunks;
+        const double done = chunks > 2 ? (c + 1 == chunks ? shares : c + 0.5) : c + 1.0;
+        const int64_t target = (c + 1 == chunks) ? total : (int64_t)((double)total * done / shares);
         int64_t e = s + 1;
         while (e < n && off[e] < target) ++e;
         out.push_back({s, e, off[s], off[e]});
@@ -171,6 +179,7 @@ RPYB_API int rpyb_signature_host(int mode, int32_t width, int32_t depth, int64_t
     RPYB_CUDA(cudaEventRecord(start_ev, cs));
     RPYB_CUDA(cudaStreamWaitEvent(cp->h2d, start_ev, 0));
     RPYB_CUDA(cudaStreamWaitEvent(cp->d2h, start_ev, 0));
+    RPYB_CUDA(cudaStreamWaitEvent(cp->comp, start_ev, 0));
 
     int status = RPYB_OK;
     for (size_t i = 0; i < ch.size() && status == RPYB_OK; ++i) {
@@ -187,15 +196,18 @@ RPYB_API int rpyb_signature_host(int mode, int32_t width, int32_t depth, int64_t
                                   (size_t)((c.r1 - c.r0) * width * es), cudaMemcpyHostToDevice,
                                   cp->h2d));
         RPYB_CUDA(cudaEventRecord(h2d_done[b], cp->h2d));
-        RPYB_CUDA(cudaStreamWaitEvent(cs, h2d_done[b], 0));
+        // consecutive chunks alternate between two compute streams, so a
+        // chunk's kernel fills the tail of the previous one
+        cudaStream_t ks = b ? cp->comp : cs;
+        RPYB_CUDA(cudaStreamWaitEvent(ks, h2d_done[b], 0));
         // output buffer b is free once chunk i-2's copy-out finished
-        if (i >= 2) RPYB_CUDA(cudaStreamWaitEvent(cs, d2h_done[b], 0));
+        if (i >= 2) RPYB_CUDA(cudaStreamWaitEvent(ks, d2h_done[b], 0));
         const int64_t* off_d = d_meta + meta_pos[i];
         const int64_t* ord_d = off_d + ns + 1;
         status = rpyb_signature(mode, width, depth, ns, off_d, inc_d, out_d, g.size(), ord_d,
-                                ws_d, (size_t)L.sig_ws_bytes, cs);
+                                ws_d, (size_t)L.sig_ws_bytes, ks);
         if (status != RPYB_OK) break;
-        RPYB_CUDA(cudaEventRecord(comp_done[b], cs));
+        RPYB_CUDA(cudaEventRecord(comp_done[b], ks));
         RPYB_CUDA(cudaStreamWaitEvent(cp->d2h, comp_done[b], 0));
         RPYB_CUDA(cudaMemcpy2DAsync(static_cast<char*>(out_host) + c.s0 * ld_out * es,
                                     (size_t)(ld_out * es), out_d, (size_t)(g.size() * es),
@@ -203,8 +215,11 @@ RPYB_API int rpyb_signature_host(int mode, int32_t width, int32_t depth, int64_t
                                     cp->d2h));
         RPYB_CUDA(cudaEventRecord(d2h_done[b], cp->d2h));
     }
-    // the caller's stream completes when the last copy-out has
+    // the caller's stream completes when the last copy-out has (which
+    // follows every kernel)
     for (int i = 0; i < 2; ++i) RPYB_CUDA(cudaStreamWaitEvent(cs, d2h_done[i], 0));
+    RPYB_CUDA(cudaEventRecord(start_ev, cp->comp));
+    RPYB_CUDA(cudaStreamWaitEvent(cs, start_ev, 0));
     for (int i = 0; i < 2; ++i) {
         cudaEventDestroy(h2d_done[i]);
         cudaEventDestroy(comp_done[i]);
