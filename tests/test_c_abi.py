@@ -50,6 +50,24 @@ def test_version_and_sizes():
     # depth out of range
     lambda L: L.rpyb_ft_exp(1, 2, 99, 1, 8, 8, 7, 7, -1, None, 0, None),
     lambda L: L.rpyb_signature(5, 2, 2, 1, 8, 8, 8, 7, None, None, 0, None),
+    # dyadic tree: null handle, bad mode, row length, support
+    lambda L: L.rpyb_dyadic_build(1, 3, 3, 2, 0.0, 1.0, 0, None, None, 3, None, None),
+    lambda L: L.rpyb_dyadic_build(9, 3, 3, 2, 0.0, 1.0, 0, None, None, 3,
+                                  ctypes.byref(ctypes.c_void_p()), None),
+    lambda L: L.rpyb_dyadic_build(1, 3, 3, 2, 0.0, 1.0, 0, None, None, 5,
+                                  ctypes.byref(ctypes.c_void_p()), None),
+    lambda L: L.rpyb_dyadic_build(1, 3, 3, 2, 1.0, 0.0, 0, None, None, 3,
+                                  ctypes.byref(ctypes.c_void_p()), None),
+    lambda L: L.rpyb_dyadic_query(None, 1, None, None, 0, None, 0, None, 0, None),
+    # piecewise query: bad shape, null intervals
+    lambda L: L.rpyb_piecewise_query(0, 3, 0, None, None, None, 0, 0.0, 1.0, 0, 1, None, None,
+                                     0, None, 0, None, 0, None),
+    lambda L: L.rpyb_piecewise_query(3, 3, 0, None, None, None, 0, 0.0, 1.0, 0, 1, None, None,
+                                     0, None, 0, None, 0, None),
+    # signature derivative: bad dtype, offsets not starting at 0
+    lambda L: L.rpyb_sig_derivative(3, 3, 3, 1, None, None, None, 6, None, 40, None, 0, None),
+    lambda L: L.rpyb_sig_derivative(1, 3, 3, 1, (ctypes.c_int64 * 2)(1, 2), None, None, 14, 8,
+                                    40, None, 0, None),
 ])
 def test_invalid_arguments_are_rejected_before_any_launch(call):
     from roughpy_b200 import _lib
@@ -62,6 +80,10 @@ def test_zero_batch_is_a_no_op():
     from roughpy_b200 import _lib
     assert _lib.lib.rpyb_ft_fma(1, 2, 2, 0, None, None, None, 7, 7, 7, None, None) == 0
     assert _lib.lib.rpyb_signature(1, 2, 2, 0, None, None, None, 7, None, None, 0, None) == 0
+    assert _lib.lib.rpyb_sig_derivative(1, 3, 3, 0, None, None, None, 14, None, 40, None, 0,
+                                        None) == 0
+    assert _lib.lib.rpyb_dyadic_free(None) == 0
+    assert _lib.lib.rpyb_release_cached_memory() == 0
 
 
 def test_python_errors_match_reference_types():
