@@ -204,6 +204,115 @@ product_kernel(const KArgs a)
     }
 }
 
+// Blocked variant for output levels k >= 2.  A thread owns the D x V words
+//   u d^(k-1) + r' d + c0 + j    (u < D first letters, j < V last letters)
+// for one middle part r' (k-2 letters) and one block c0 .. c0+V-1 of last
+// letters.  For a split point 1 <= p <= k-1 the D left-factor words
+// (u, r'_1 .. r'_{p-1}) do not depend on the last letter and the V
+// right-factor words (r'_{p..k-2}, c) do not depend on the first, so D + V
+// loads feed D V FMAs; the top-level words of the p = k and p = 0 terms are
+// read as runs of V consecutive words.
+template <typename T, typename TR, int D, int V, int ACC = 0>
+__global__ void __launch_bounds__(kThreads)
+product_kernel_blocked(const KArgs a)
+{
+    constexpr int NB = D / V;
+    using AccT = typename AccSel<T, ACC>::type;
+    const int64_t f_begin = (int64_t)blockIdx.x * a.tile_r;
+    const int64_t f_end = min(f_begin + a.tile_r, a.ftotal);
+
+    for (int64_t b = blockIdx.y; b < a.batch; b += gridDim.y) {
+        const int64_t ro = a.out_idx ? a.out_idx[b] : b;
+        const int64_t rl = a.lhs_idx ? a.lhs_idx[b] : b;
+        const int64_t rr = a.rhs_idx ? a.rhs_idx[b] : b;
+        T* __restrict__ out = static_cast<T*>(a.out) + ro * a.ld_out;
+        const T* __restrict__ lhs = static_cast<const T*>(a.lhs) + rl * a.ld_lhs;
+        const TR* __restrict__ rhs = static_cast<const TR*>(a.rhs) + rr * a.ld_rhs;
+        const T* __restrict__ add =
+            a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
+        const T lhs0 = (a.lhs0_from_mem ? __ldg(lhs) : T(0)) + T(a.lhs0_add);
+        const T rhs0 = T(__ldg(rhs));
+
+        for (int64_t f = f_begin + threadIdx.x; f < f_end; f += kThreads) {
+            int k = a.klo;
+            while (f >= a.fcum[k + 1]) ++k;
+            const int64_t unit = f - a.fcum[k];
+            const uint32_t rp = (uint32_t)(unit / NB);
+            const int c0 = (int)(unit - (int64_t)rp * NB) * V;
+            const int64_t dk1 = a.pw[k - 1];
+            const int64_t obase = a.db[k] + (int64_t)rp * D + c0;
+
+            AccT acc[D][V];
+#pragma unroll
+            for (int u = 0; u < D; ++u)
+#pragma unroll
+                for (int j = 0; j < V; ++j)
+                    acc[u][j].init(a.accumulate ? out[obase + u * dk1 + j] : T(0));
+
+            const int pmax = a.pmax[k];
+            const int pmin = a.pmin[k];
+            if (pmax >= pmin) {
+                if (k <= pmax && k >= pmin) {
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j)
+                            acc[u][j].add(__ldg(lhs + obase + u * dk1 + j), rhs0);
+                }
+                // split p = k - s: left word (u, r'_1..r'_{p-1}) = u d^(p-1) + q,
+                // right word (r'_p..r'_{k-2}, c) = m d + c with q, m peeled from r'
+                uint32_t q = rp;
+                uint32_t m = 0;
+                for (int s = 1; s <= k - 1; ++s) {
+                    const int p = k - s;
+                    if (p <= pmax && p >= pmin) {
+                        T lv[D];
+                        T rv[V];
+                        const T* lp = lhs + a.db[p] + q;
+                        const uint32_t dp1 = (uint32_t)a.pw[p - 1];
+#pragma unroll
+                        for (int u = 0; u < D; ++u) lv[u] = __ldg(lp + u * dp1);
+                        const TR* rq = rhs + a.db[s] + (int64_t)m * D + c0;
+#pragma unroll
+                        for (int j = 0; j < V; ++j) rv[j] = T(__ldg(rq + j));
+#pragma unroll
+                        for (int u = 0; u < D; ++u)
+#pragma unroll
+                            for (int j = 0; j < V; ++j) acc[u][j].add(lv[u], rv[j]);
+                    }
+                    const uint32_t q2 = q / (uint32_t)D;
+                    m += (q - q2 * (uint32_t)D) * (uint32_t)a.pw[s - 1];
+                    q = q2;
+                }
+                if (pmin <= 0 && pmax >= 0) {
+                    const TR* rk = rhs + obase;
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j)
+                            acc[u][j].add(lhs0, T(__ldg(rk + u * dk1 + j)));
+                }
+            }
+
+            const T sc = T(a.scale[k]);
+#pragma unroll
+            for (int u = 0; u < D; ++u)
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const int64_t o = obase + u * dk1 + j;
+                    T v;
+                    if (a.accumulate) {
+                        v = acc[u][j].value();
+                    } else {
+                        v = sc * acc[u][j].value();
+                        if (add) v += add[o];
+                    }
+                    out[o] = v;
+                }
+        }
+    }
+}
+
 template <typename TD, typename TS>
 __global__ void convert_rows_kernel(TD* dst, int64_t ld_dst, const TS* src, int64_t ld_src,
                                     int64_t cols, int64_t batch)
@@ -259,12 +368,74 @@ int tile_words()
     return w;
 }
 
+// Width -> last-letter block V of the blocked kernel (0: not used)
+int blocked_v(int width)
+{
+    switch (width) {
+        case 2: return 2;
+        case 3: return 3;
+        case 4: return 4;
+        case 5: return 5;
+        case 6: return 3;
+        case 8: return 4;
+        default: return 0;
+    }
+}
+
+// RPYB_PRODUCT_BLOCKED=0 keeps every level on the suffix kernel
+bool blocked_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("RPYB_PRODUCT_BLOCKED");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename T, typename TR, int ACC>
+int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
+{
+    switch (a.width) {
+        case 2: product_kernel_blocked<T, TR, 2, 2, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 3: product_kernel_blocked<T, TR, 3, 3, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 4: product_kernel_blocked<T, TR, 4, 4, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 5: product_kernel_blocked<T, TR, 5, 5, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6: product_kernel_blocked<T, TR, 6, 3, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        case 8: product_kernel_blocked<T, TR, 8, 4, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        default: return fail(RPYB_E_UNSUPPORTED, "no blocked product kernel for this width");
+    }
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
 }  // namespace
+
+static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
+                         const ProductRows& rows, cudaStream_t stream, bool blocked);
 
 int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
                    const ProductRows& rows, cudaStream_t stream)
 {
     if (rows.batch <= 0) return RPYB_OK;
+    const int V = blocked_enabled() ? blocked_v(g.width) : 0;
+    const int kb = std::max(2, spec.klo);
+    if (V == 0 || spec.khi < kb) return launch_levels(dtype, g, spec, rows, stream, false);
+    // levels 0..1 (and the level-0 rule) by the suffix kernel, levels >= 2 blocked
+    int rc;
+    if (spec.klo <= 1 || spec.l0_write) {
+        ProductSpec lo = spec;
+        lo.khi = std::min(spec.khi, 1);
+        if ((rc = launch_levels(dtype, g, lo, rows, stream, false))) return rc;
+    }
+    ProductSpec hi = spec;
+    hi.klo = kb;
+    hi.l0_write = false;
+    return launch_levels(dtype, g, hi, rows, stream, true);
+}
+
+static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
+                         const ProductRows& rows, cudaStream_t stream, bool blocked)
+{
     KArgs a{};
     a.width = g.width;
     a.klo = std::max(1, spec.klo);
@@ -273,9 +444,12 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
     for (int i = 0; i <= kMaxDepth; ++i) a.pw[i] = g.pw[i];
     int64_t f = 0;
     for (int k = 0; k <= kMaxDepth + 1; ++k) a.fcum[k] = 0;
+    // work units per level: suffixes (one per d^(k-1)) or, blocked, one per
+    // middle part and last-letter block (d^(k-2) * d / V)
+    const int V = blocked ? blocked_v(g.width) : 0;
     for (int k = a.klo; k <= a.khi; ++k) {
         a.fcum[k] = f;
-        f += g.pw[k - 1];
+        f += blocked ? g.pw[k - 2] * (g.width / V) : g.pw[k - 1];
     }
     // sentinel entries above khi so the level search stops
     for (int k = std::max(a.khi + 1, a.klo); k <= kMaxDepth + 1; ++k) a.fcum[k] = f;
@@ -306,13 +480,23 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
     a.rhs_idx = rows.rhs_idx;
     a.batch = rows.batch;
 
-    // Suffixes per tile: about kTileWords output words per CTA (at least one
-    // suffix per thread).
-    a.tile_r = std::max<int64_t>(kThreads, tile_words() / std::max(1, g.width));
+    // Work units per tile: about kTileWords output words per CTA (at least
+    // one unit per thread).
+    const int64_t words_per_unit = blocked ? (int64_t)g.width * V : g.width;
+    a.tile_r = std::max<int64_t>(kThreads, tile_words() / std::max<int64_t>(1, words_per_unit));
     int64_t tiles = (a.ftotal + a.tile_r - 1) / a.tile_r;
     if (tiles == 0) tiles = 1;  // level 0 only
     if (tiles > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "tensor too large");
     dim3 grid((unsigned)tiles, (unsigned)std::min<int64_t>(rows.batch, 65535), 1);
+    if (blocked) {
+        if (dtype == RPYB_F64) return dispatch_blocked<double, double, 0>(a, grid, stream);
+        if (dtype == kMixedF64F32) return dispatch_blocked<double, float, 0>(a, grid, stream);
+        switch (f32_acc_mode()) {
+            case 1: return dispatch_blocked<float, float, 1>(a, grid, stream);
+            case 2: return dispatch_blocked<float, float, 2>(a, grid, stream);
+            default: return dispatch_blocked<float, float, 0>(a, grid, stream);
+        }
+    }
     if (dtype == RPYB_F64) return dispatch<double, double, 0>(a, grid, stream);
     if (dtype == kMixedF64F32) return dispatch<double, float, 0>(a, grid, stream);
     switch (f32_acc_mode()) {
