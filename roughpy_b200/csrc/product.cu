@@ -212,8 +212,8 @@ product_kernel(const KArgs a)
 // right-factor words (r'_{p..k-2}, c) do not depend on the first, so D + V
 // loads feed D V FMAs; the top-level words of the p = k and p = 0 terms are
 // read as runs of V consecutive words.
-template <typename T, typename TR, int D, int V, int ACC = 0>
-__global__ void __launch_bounds__(kThreads)
+template <typename T, typename TR, int D, int V, int ACC = 0, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB)
 product_kernel_blocked(const KArgs a)
 {
     constexpr int NB = D / V;
@@ -377,7 +377,7 @@ int blocked_v(int width)
         case 4: return 4;
         case 5: return 5;
         case 6: return 3;
-        case 8: return 4;
+        case 8: return 2;
         default: return 0;
     }
 }
@@ -396,12 +396,14 @@ template <typename T, typename TR, int ACC>
 int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
 {
     switch (a.width) {
-        case 2: product_kernel_blocked<T, TR, 2, 2, ACC><<<grid, kThreads, 0, stream>>>(a); break;
-        case 3: product_kernel_blocked<T, TR, 3, 3, ACC><<<grid, kThreads, 0, stream>>>(a); break;
-        case 4: product_kernel_blocked<T, TR, 4, 4, ACC><<<grid, kThreads, 0, stream>>>(a); break;
-        case 5: product_kernel_blocked<T, TR, 5, 5, ACC><<<grid, kThreads, 0, stream>>>(a); break;
-        case 6: product_kernel_blocked<T, TR, 6, 3, ACC><<<grid, kThreads, 0, stream>>>(a); break;
-        case 8: product_kernel_blocked<T, TR, 8, 4, ACC><<<grid, kThreads, 0, stream>>>(a); break;
+        // last-letter blocks and resident blocks per SM (register caps) from
+        // measurements on B200
+        case 2: product_kernel_blocked<T, TR, 2, 2, ACC, 5><<<grid, kThreads, 0, stream>>>(a); break;
+        case 3: product_kernel_blocked<T, TR, 3, 3, ACC, 4><<<grid, kThreads, 0, stream>>>(a); break;
+        case 4: product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6: product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 8: product_kernel_blocked<T, TR, 8, 2, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
         default: return fail(RPYB_E_UNSUPPORTED, "no blocked product kernel for this width");
     }
     RPYB_CUDA(cudaGetLastError());
