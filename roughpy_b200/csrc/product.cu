@@ -204,7 +204,7 @@ product_kernel(const KArgs a)
     }
 }
 
-// Blocked variant for output levels k >= 2.  A thread owns the D x V words
+// Blocked variant for output levels k >= 2 (one owned last letter).  A thread owns the D x V words
 //   u d^(k-1) + r' d + c0 + j    (u < D first letters, j < V last letters)
 // for one middle part r' (k-2 letters) and one block c0 .. c0+V-1 of last
 // letters.  For a split point 1 <= p <= k-1 the D left-factor words
@@ -313,6 +313,129 @@ product_kernel_blocked(const KArgs a)
     }
 }
 
+// Blocked variant owning the last L >= 2 letters (V = D^L combinations): a
+// thread computes the D x V words u d^(k-1) + r' V + j for one middle part
+// r' (k-1-L letters), for output levels k > L.  Split points with a right
+// part of s >= L letters share D left words and V right words as above;
+// the s < L splits cut into the owned letters and load D d^(L-s) left and
+// d^s right words.
+template <typename T, typename TR, int D, int L, int ACC = 0, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB)
+product_kernel_blocked_l(const KArgs a)
+{
+    constexpr int V = (L == 2) ? D * D : D * D * D;
+    using AccT = typename AccSel<T, ACC>::type;
+    const int64_t f_begin = (int64_t)blockIdx.x * a.tile_r;
+    const int64_t f_end = min(f_begin + a.tile_r, a.ftotal);
+
+    for (int64_t b = blockIdx.y; b < a.batch; b += gridDim.y) {
+        const int64_t ro = a.out_idx ? a.out_idx[b] : b;
+        const int64_t rl = a.lhs_idx ? a.lhs_idx[b] : b;
+        const int64_t rr = a.rhs_idx ? a.rhs_idx[b] : b;
+        T* __restrict__ out = static_cast<T*>(a.out) + ro * a.ld_out;
+        const T* __restrict__ lhs = static_cast<const T*>(a.lhs) + rl * a.ld_lhs;
+        const TR* __restrict__ rhs = static_cast<const TR*>(a.rhs) + rr * a.ld_rhs;
+        const T* __restrict__ add =
+            a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
+        const T lhs0 = (a.lhs0_from_mem ? __ldg(lhs) : T(0)) + T(a.lhs0_add);
+        const T rhs0 = T(__ldg(rhs));
+
+        for (int64_t f = f_begin + threadIdx.x; f < f_end; f += kThreads) {
+            int k = a.klo;
+            while (f >= a.fcum[k + 1]) ++k;
+            const uint32_t rp = (uint32_t)(f - a.fcum[k]);
+            const int64_t dk1 = a.pw[k - 1];
+            const int64_t obase = a.db[k] + (int64_t)rp * V;
+
+            AccT acc[D][V];
+#pragma unroll
+            for (int u = 0; u < D; ++u)
+#pragma unroll
+                for (int j = 0; j < V; ++j)
+                    acc[u][j].init(a.accumulate ? out[obase + u * dk1 + j] : T(0));
+
+            const int pmax = a.pmax[k];
+            const int pmin = a.pmin[k];
+            if (pmax >= pmin) {
+                if (k <= pmax && k >= pmin) {
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j)
+                            acc[u][j].add(__ldg(lhs + obase + u * dk1 + j), rhs0);
+                }
+                // splits cutting into the owned letters: right part j mod D^s
+#pragma unroll
+                for (int s = 1; s < L; ++s) {
+                    const int p = k - s;
+                    if (p <= pmax && p >= pmin) {
+                        constexpr int dummy = 0;
+                        (void)dummy;
+                        const int ds = (s == 1) ? D : D * D;          // D^s (L <= 3)
+                        const int dl = V / ds;                          // D^(L-s)
+                        const uint32_t dp1 = (uint32_t)a.pw[p - 1];
+                        const T* lp = lhs + a.db[p] + (int64_t)rp * dl;
+                        const TR* rq = rhs + a.db[s];
+#pragma unroll
+                        for (int u = 0; u < D; ++u)
+#pragma unroll
+                            for (int j = 0; j < V; ++j)
+                                acc[u][j].add(__ldg(lp + u * dp1 + j / ds), T(__ldg(rq + j % ds)));
+                    }
+                }
+                // splits with a right part of s >= L letters
+                uint32_t q = rp;
+                uint32_t m = 0;
+                for (int s = L; s <= k - 1; ++s) {
+                    const int p = k - s;
+                    if (p <= pmax && p >= pmin) {
+                        T lv[D];
+                        T rv[V];
+                        const T* lp = lhs + a.db[p] + q;
+                        const uint32_t dp1 = (uint32_t)a.pw[p - 1];
+#pragma unroll
+                        for (int u = 0; u < D; ++u) lv[u] = __ldg(lp + u * dp1);
+                        const TR* rq = rhs + a.db[s] + (int64_t)m * V;
+#pragma unroll
+                        for (int j = 0; j < V; ++j) rv[j] = T(__ldg(rq + j));
+#pragma unroll
+                        for (int u = 0; u < D; ++u)
+#pragma unroll
+                            for (int j = 0; j < V; ++j) acc[u][j].add(lv[u], rv[j]);
+                    }
+                    const uint32_t q2 = q / (uint32_t)D;
+                    m += (q - q2 * (uint32_t)D) * (uint32_t)a.pw[s - L];
+                    q = q2;
+                }
+                if (pmin <= 0 && pmax >= 0) {
+                    const TR* rk = rhs + obase;
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j)
+                            acc[u][j].add(lhs0, T(__ldg(rk + u * dk1 + j)));
+                }
+            }
+
+            const T sc = T(a.scale[k]);
+#pragma unroll
+            for (int u = 0; u < D; ++u)
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const int64_t o = obase + u * dk1 + j;
+                    T v;
+                    if (a.accumulate) {
+                        v = acc[u][j].value();
+                    } else {
+                        v = sc * acc[u][j].value();
+                        if (add) v += add[o];
+                    }
+                    out[o] = v;
+                }
+        }
+    }
+}
+
 template <typename TD, typename TS>
 __global__ void convert_rows_kernel(TD* dst, int64_t ld_dst, const TS* src, int64_t ld_src,
                                     int64_t cols, int64_t batch)
@@ -368,11 +491,10 @@ int tile_words()
     return w;
 }
 
-// Width -> last-letter block V of the blocked kernel (0: not used)
-int blocked_v(int width)
+// Width -> last-letter block V of the one-letter blocked kernel (0: none)
+int blocked_v_one(int width)
 {
     switch (width) {
-        case 2: return 2;
         case 3: return 3;
         case 4: return 4;
         case 5: return 5;
@@ -380,6 +502,31 @@ int blocked_v(int width)
         case 8: return 2;
         default: return 0;
     }
+}
+
+// Width 2 owns its last 2 letters (RPYB_W2_LETTERS=3: three; two measured
+// faster on B200)
+int width2_letters()
+{
+    static const int l = [] {
+        const char* e = getenv("RPYB_W2_LETTERS");
+        return (e && e[0] == '3') ? 3 : 2;
+    }();
+    return l;
+}
+
+// Width -> number of owned last letters of the blocked kernels (0: none)
+int blocked_l(int width)
+{
+    if (width == 2) return width2_letters();
+    return blocked_v_one(width) ? 1 : 0;
+}
+
+// Width -> owned last-letter combinations V per thread
+int blocked_v(int width)
+{
+    if (width == 2) return width2_letters() == 2 ? 4 : 8;
+    return blocked_v_one(width);
 }
 
 // RPYB_PRODUCT_BLOCKED=0 keeps every level on the suffix kernel
@@ -395,10 +542,17 @@ bool blocked_enabled()
 template <typename T, typename TR, int ACC>
 int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
 {
+    if (a.width == 2) {
+        if (width2_letters() == 2)
+            product_kernel_blocked_l<T, TR, 2, 2, ACC, 5><<<grid, kThreads, 0, stream>>>(a);
+        else
+            product_kernel_blocked_l<T, TR, 2, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+        RPYB_CUDA(cudaGetLastError());
+        return RPYB_OK;
+    }
     switch (a.width) {
         // last-letter blocks and resident blocks per SM (register caps) from
         // measurements on B200
-        case 2: product_kernel_blocked<T, TR, 2, 2, ACC, 5><<<grid, kThreads, 0, stream>>>(a); break;
         case 3: product_kernel_blocked<T, TR, 3, 3, ACC, 4><<<grid, kThreads, 0, stream>>>(a); break;
         case 4: product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
         case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
@@ -419,14 +573,14 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
                    const ProductRows& rows, cudaStream_t stream)
 {
     if (rows.batch <= 0) return RPYB_OK;
-    const int V = blocked_enabled() ? blocked_v(g.width) : 0;
-    const int kb = std::max(2, spec.klo);
-    if (V == 0 || spec.khi < kb) return launch_levels(dtype, g, spec, rows, stream, false);
-    // levels 0..1 (and the level-0 rule) by the suffix kernel, levels >= 2 blocked
+    const int L = blocked_enabled() ? blocked_l(g.width) : 0;
+    const int kb = std::max(L + 1, spec.klo);
+    if (L == 0 || spec.khi < kb) return launch_levels(dtype, g, spec, rows, stream, false);
+    // levels 0..L (and the level-0 rule) by the suffix kernel, the rest blocked
     int rc;
-    if (spec.klo <= 1 || spec.l0_write) {
+    if (spec.klo <= L || spec.l0_write) {
         ProductSpec lo = spec;
-        lo.khi = std::min(spec.khi, 1);
+        lo.khi = std::min(spec.khi, L);
         if ((rc = launch_levels(dtype, g, lo, rows, stream, false))) return rc;
     }
     ProductSpec hi = spec;
@@ -449,9 +603,12 @@ static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
     // work units per level: suffixes (one per d^(k-1)) or, blocked, one per
     // middle part and last-letter block (d^(k-2) * d / V)
     const int V = blocked ? blocked_v(g.width) : 0;
+    const int L = blocked ? blocked_l(g.width) : 0;
     for (int k = a.klo; k <= a.khi; ++k) {
         a.fcum[k] = f;
-        f += blocked ? g.pw[k - 2] * (g.width / V) : g.pw[k - 1];
+        if (!blocked) f += g.pw[k - 1];
+        else if (L == 1) f += g.pw[k - 2] * (g.width / V);
+        else f += g.pw[k - 1 - L];
     }
     // sentinel entries above khi so the level search stops
     for (int k = std::max(a.khi + 1, a.klo); k <= kMaxDepth + 1; ++k) a.fcum[k] = f;
