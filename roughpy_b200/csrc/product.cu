@@ -491,12 +491,13 @@ int tile_words()
     return w;
 }
 
-// Width -> last-letter block V of the one-letter blocked kernel (0: none)
-int blocked_v_one(int width)
+// Width -> last-letter block V of the one-letter blocked kernel (0: none);
+// float64 rows at width 4 use a block of 2 (more resident warps)
+int blocked_v_one(int width, bool f64 = false)
 {
     switch (width) {
         case 3: return 3;
-        case 4: return 4;
+        case 4: return f64 ? 2 : 4;
         case 5: return 5;
         case 6: return 3;
         case 8: return 2;
@@ -523,10 +524,10 @@ int blocked_l(int width)
 }
 
 // Width -> owned last-letter combinations V per thread
-int blocked_v(int width)
+int blocked_v(int width, bool f64)
 {
     if (width == 2) return width2_letters() == 2 ? 4 : 8;
-    return blocked_v_one(width);
+    return blocked_v_one(width, f64);
 }
 
 // RPYB_PRODUCT_BLOCKED=0 keeps every level on the suffix kernel
@@ -554,7 +555,12 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
         // last-letter blocks and resident blocks per SM (register caps) from
         // measurements on B200
         case 3: product_kernel_blocked<T, TR, 3, 3, ACC, 4><<<grid, kThreads, 0, stream>>>(a); break;
-        case 4: product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 4:
+            if (sizeof(T) == 8)
+                product_kernel_blocked<T, TR, 4, 2, ACC, 4><<<grid, kThreads, 0, stream>>>(a);
+            else
+                product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+            break;
         case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
         case 6: product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
         case 8: product_kernel_blocked<T, TR, 8, 2, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
@@ -602,7 +608,7 @@ static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
     for (int k = 0; k <= kMaxDepth + 1; ++k) a.fcum[k] = 0;
     // work units per level: suffixes (one per d^(k-1)) or, blocked, one per
     // middle part and last-letter block (d^(k-2) * d / V)
-    const int V = blocked ? blocked_v(g.width) : 0;
+    const int V = blocked ? blocked_v(g.width, dtype != RPYB_F32) : 0;
     const int L = blocked ? blocked_l(g.width) : 0;
     for (int k = a.klo; k <= a.khi; ++k) {
         a.fcum[k] = f;
