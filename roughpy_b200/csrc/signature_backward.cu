@@ -19,8 +19,8 @@
 // Lane kernel (widths 2..8 with width^(depth-2) <= 992): one block per
 // stream, one thread ("lane") per level-(N-2) word pi.  A lane keeps S_t on
 // its prefix path and on pi's D children (levels <= N-1; the top level of S
-// is never needed) and G on pi and its children, all in float64 registers;
-// the constant top level of G sits in shared memory.  S_t is recovered from
+// is never needed) and G on pi in float64 registers, and G on pi's children
+// in shared memory next to the constant top level of G.  S_t is recovered from
 // S_{t+1} by the inverse step S_t = S_{t+1} (x) exp(-x_t) and re-anchored to
 // a forward checkpoint every K steps.  The lanes' subtree terms need no
 // communication.  Up to four extra "fold" warps per block trail the lanes by
@@ -308,14 +308,15 @@ struct LaneLayout {
     // shared memory: per hand-off buffer b < NB the lane warps' gradient
     // partials, the fold warps' partials, the lanes' M vectors and the states
     // of shared prefixes; then fold-private ancestor data, the staged
-    // increments and the top-level adjoints
+    // increments, the top-level adjoints and the lanes' child adjoints G[pi m]
+    // (kept here rather than in registers, which the fold warps cap)
     __host__ __device__ static constexpr int64_t per_buf()
     {
         return NWARP * 8 * 8 + NF * 8 * 8 + align16(n_mlev * 8) + align16(n_anc * 8);
     }
     __host__ __device__ static constexpr int64_t fixed()
     {
-        return align16(n_mbuf * 8) + align16(n_anc * 8) + align16((int64_t)CH * D * 8) +
+        return align16(D * W * 8) + align16(n_mbuf * 8) + align16(n_anc * 8) + align16((int64_t)CH * D * 8) +
                align16((int64_t)CH * D * (int64_t)sizeof(T)) +
                (GT_SMEM ? align16(TOPW * (int64_t)sizeof(T)) : 0);
     }
@@ -329,7 +330,8 @@ struct LaneLayout {
     static constexpr int64_t o_xd = o_ganc + align16(n_anc * 8);          // f64 [CH][D]
     static constexpr int64_t o_xt = o_xd + align16((int64_t)CH * D * 8);  // T [CH][D]
     static constexpr int64_t o_gtop = o_xt + align16((int64_t)CH * D * (int64_t)sizeof(T));
-    static constexpr int64_t bytes = o_gtop + (GT_SMEM ? align16(TOPW * (int64_t)sizeof(T)) : 0);
+    static constexpr int64_t o_gms = o_gtop + (GT_SMEM ? align16(TOPW * (int64_t)sizeof(T)) : 0);
+    static constexpr int64_t bytes = o_gms + align16(D * W * 8);
     static constexpr int64_t mlev_stride = align16(n_mlev * 8) / 8;
     static constexpr int64_t sanc_stride = align16(n_anc * 8) / 8;
     // named barriers (0 is __syncthreads): lanes filled buffer b, fold warps
@@ -497,6 +499,7 @@ signature_backward_lanes(const BwdArgs a)
     double* xd = reinterpret_cast<double*>(smem_raw + LY::o_xd);
     T* xt = reinterpret_cast<T*>(smem_raw + LY::o_xt);
     T* gtop_s = reinterpret_cast<T*>(smem_raw + LY::o_gtop);
+    double* gms = reinterpret_cast<double*>(smem_raw + LY::o_gms);
     __shared__ int s_item;
 
     const int tid = (int)threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -580,9 +583,10 @@ signature_backward_lanes(const BwdArgs a)
 
         // ---- adjoint state from the upstream gradient
         double gp = (double)gsig[LY::db(P > 0 ? P : 0) + pi];
-        double gm[D];
+        if (active) {
 #pragma unroll
-        for (int m = 0; m < D; ++m) gm[m] = (double)gsig[LY::db(N - 1) + (int64_t)pi * D + m];
+            for (int m = 0; m < D; ++m) gms[m * W + pi] = (double)gsig[LY::db(N - 1) + (int64_t)pi * D + m];
+        }
         if constexpr (GT_SMEM) {
             for (int64_t i = tid; i < LY::TOPW; i += NTB) {
                 const int64_t l = i / (D * D);
@@ -676,10 +680,11 @@ signature_backward_lanes(const BwdArgs a)
 #pragma unroll
                         for (int b = 0; b < D; ++b) gx[b] = fma(f, g[b], gx[b]);
                         const double yd = (double)y;                        // M_1(pi m)
-                        gx[m] += (T)fma(F0pi, gm[m], F1pi * yd);
-                        M1 = fma(x[m], gm[m], M1);
+                        const double gmv = gms[m * W + pi];
+                        gx[m] += (T)fma(F0pi, gmv, F1pi * yd);
+                        M1 = fma(x[m], gmv, M1);
                         M2 = fma(x[m], yd, M2);
-                        gm[m] += yd;
+                        if (active) gms[m * W + pi] = gmv + yd;
                     }
                     const double M0 = gp;
                     if constexpr (P >= 1) {
