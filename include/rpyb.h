@@ -303,6 +303,20 @@ RPYB_API int rpyb_sparse_map(int dtype, int64_t n_rows, int64_t n_cols, int64_t 
                              int64_t ld_y, int64_t ld_x, double scale, void* stream);
 
 /*
+ * Batched tensor -> Lie (Hall coordinates, rbracketing / degree) and
+ * Lie -> tensor maps with the maps kept on the device (uploaded once per
+ * device and shape).  Both assign their output rows.
+ * Replaces: roughpy/compute/_src/dense_basic.cpp:1055-1150
+ *           (py_dense_tensor_to_lie) and :564-620 (py_dense_lie_to_tensor),
+ *           i.e. Context::tensor_to_lie / lie_to_tensor
+ *           (algebra/include/roughpy/algebra/context.h:171-172).
+ */
+RPYB_API int rpyb_tensor_to_lie(int dtype, int32_t width, int32_t depth, int64_t batch, void* out,
+                                int64_t ld_out, const void* arg, int64_t ld_arg, void* stream);
+RPYB_API int rpyb_lie_to_tensor(int dtype, int32_t width, int32_t depth, int64_t batch, void* out,
+                                int64_t ld_out, const void* arg, int64_t ld_arg, void* stream);
+
+/*
  * Dissection of the clopen interval [inf, sup) into maximal dyadic pieces at
  * resolution `tol`, in order.  Piece i is [k[i] / 2^p[i], (k[i]+1) / 2^p[i]).
  * Writes at most `cap` pieces and returns the number of pieces (which may

@@ -80,6 +80,8 @@ SIGNATURES = {
     "rpyb_lie_map_csr": (_i64, [_i32, _i32, _int, _pi64, _pi64, _pdbl]),
     "rpyb_sparse_map": (_int, [_int, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _dbl,
                                _vp]),
+    "rpyb_tensor_to_lie": (_int, [_int, _i32, _i32, _i64, _vp, _i64, _vp, _i64, _vp]),
+    "rpyb_lie_to_tensor": (_int, [_int, _i32, _i32, _i64, _vp, _i64, _vp, _i64, _vp]),
     "rpyb_dyadic_dissect": (_i64, [_dbl, _dbl, _i32, _int, _vp, _vp, _i64]),
     "rpyb_dyadic_dissect_batch": (_int, [_i64, _vp, _vp, _vp, _int, _vp, _vp, _i64, _vp]),
     "rpyb_dyadic_build": (_int, [_int, _i32, _i32, _i32, _dbl, _dbl, _i64, _vp, _vp, _i32, _vp,

@@ -304,3 +304,54 @@ int refine_and_dissect(int64_t n, const double* inf, const double* sup, double s
 }
 
 }  // namespace rpyb
+
+using namespace rpyb;
+
+extern "C" {
+
+RPYB_API int rpyb_tensor_to_lie(int dtype, int32_t width, int32_t depth, int64_t batch, void* out,
+                                int64_t ld_out, const void* arg, int64_t ld_arg, void* stream)
+{
+    int rc;
+    if (dtype != RPYB_F32 && dtype != RPYB_F64) return fail(RPYB_E_INVALID, "unsupported dtype");
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    if (batch < 0) return fail(RPYB_E_INVALID, "negative batch");
+    if (batch == 0) return RPYB_OK;
+    if (!out || !arg) return fail(RPYB_E_INVALID, "null pointer");
+    const int64_t L = rpyb_lie_basis_size(width, depth);
+    if (L < 0) return (int)L;
+    if (ld_out < L || ld_arg < g.size()) return fail(RPYB_E_INVALID, "row stride too small");
+    const LieMapsDev* maps = nullptr;
+    if ((rc = lie_maps_device(g, &maps))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t es = dtype == RPYB_F64 ? 8 : 4;
+    RPYB_CUDA(cudaMemset2DAsync(out, (size_t)ld_out * es, 0, (size_t)L * es, (size_t)batch, s));
+    return rpyb_sparse_map(dtype, L, g.size(), batch, maps->t2l_ptr, maps->t2l_idx, maps->t2l_val,
+                           out, arg, ld_out, ld_arg, 1.0, s);
+}
+
+RPYB_API int rpyb_lie_to_tensor(int dtype, int32_t width, int32_t depth, int64_t batch, void* out,
+                                int64_t ld_out, const void* arg, int64_t ld_arg, void* stream)
+{
+    int rc;
+    if (dtype != RPYB_F32 && dtype != RPYB_F64) return fail(RPYB_E_INVALID, "unsupported dtype");
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    if (batch < 0) return fail(RPYB_E_INVALID, "negative batch");
+    if (batch == 0) return RPYB_OK;
+    if (!out || !arg) return fail(RPYB_E_INVALID, "null pointer");
+    const int64_t L = rpyb_lie_basis_size(width, depth);
+    if (L < 0) return (int)L;
+    if (ld_out < g.size() || ld_arg < L) return fail(RPYB_E_INVALID, "row stride too small");
+    const LieMapsDev* maps = nullptr;
+    if ((rc = lie_maps_device(g, &maps))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t es = dtype == RPYB_F64 ? 8 : 4;
+    RPYB_CUDA(cudaMemset2DAsync(out, (size_t)ld_out * es, 0, (size_t)g.size() * es, (size_t)batch,
+                                s));
+    return rpyb_sparse_map(dtype, g.size(), L, batch, maps->l2t_ptr, maps->l2t_idx, maps->l2t_val,
+                           out, arg, ld_out, ld_arg, 1.0, s);
+}
+
+}  // extern "C"

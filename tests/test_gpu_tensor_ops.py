@@ -168,3 +168,38 @@ def test_lie_maps_on_gpu(golden):
         np.testing.assert_allclose(got, g[f"{t}_l2t_out"], rtol=0, atol=1e-12)
         got = rpc.tensor_to_lie(rpc.FreeTensor(g[f"{t}_t2l_in"], tb), lb).data
         np.testing.assert_allclose(got, g[f"{t}_t2l_out"], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("w,d", [(4, 4), (3, 5), (8, 3)])
+def test_c_abi_tensor_lie_maps(w, d):
+    """rpyb_tensor_to_lie / rpyb_lie_to_tensor (device-cached maps, assigning
+    outputs) equal the roughpy.compute-style dense maps, and t2l(l2t(x)) = x
+    on Lie elements; float32 rows within 1e-6."""
+    import torch
+    from roughpy_b200 import _lib
+    from roughpy_b200 import compute as rpc
+    lb, tb = rpc.LieBasis(w, d), rpc.TensorBasis(w, d)
+    L, T = lb.size(), tb.size()
+    rng = np.random.default_rng(w * 5 + d)
+    x = torch.from_numpy(rng.normal(size=(7, L))).cuda()
+    emb = torch.full((7, T), 3.0, dtype=torch.float64, device="cuda")   # overwritten
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check(_lib.lib.rpyb_lie_to_tensor(_lib.F64, w, d, 7, emb.data_ptr(), T, x.data_ptr(), L, s))
+    want = torch.zeros((7, T), dtype=torch.float64, device="cuda")
+    rpc._internals.dense_lie_to_tensor(want, x, lb.get_l2t_matrix(), lb, tb)
+    assert float((emb - want).abs().max()) <= 1e-14 * float(want.abs().max())
+    back = torch.full((7, L), -1.0, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F64, w, d, 7, back.data_ptr(), L, emb.data_ptr(), T,
+                                           s))
+    assert float((back - x).abs().max()) <= 1e-13 * float(x.abs().max())
+    t = torch.from_numpy(rng.normal(size=(5, T))).cuda()
+    got = torch.empty((5, L), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F64, w, d, 5, got.data_ptr(), L, t.data_ptr(), T, s))
+    ref = torch.zeros((5, L), dtype=torch.float64, device="cuda")
+    rpc._internals.dense_tensor_to_lie(ref, t, lb.get_t2l_matrix(), lb, tb)
+    assert float((got - ref).abs().max()) <= 1e-14 * float(ref.abs().max())
+    t32 = t.float()
+    got32 = torch.empty((5, L), dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F32, w, d, 5, got32.data_ptr(), L, t32.data_ptr(), T,
+                                           s))
+    assert float((got32.double() - ref).abs().max()) <= 1e-6 * float(ref.abs().max())
