@@ -1,6 +1,7 @@
 // Shared stream building blocks (see stream_ops.cuh).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -72,6 +73,42 @@ int upload_csr(const Geometry& g, int which, int64_t n_rows, const int64_t** ptr
     *ptr = dp;
     *idx = di;
     *val = dv;
+    return RPYB_OK;
+}
+
+// Pinned staging for host -> device uploads of index lists.  A copy from
+// pageable memory makes cudaMemcpyAsync wait for the stream, which would
+// serialise the host work of the next query chunk behind the device work of
+// the previous one.  Two pinned buffers per host thread and device
+// alternate; an event per buffer marks when its last copy has completed.
+struct PinnedStage {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+};
+
+int upload_async(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    thread_local PinnedStage stages[64][2];
+    thread_local int next[64] = {};
+    int dev = 0;
+    RPYB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(RPYB_E_UNSUPPORTED, "device ordinal too large");
+    PinnedStage& st = stages[dev][next[dev]];
+    next[dev] ^= 1;
+    if (st.ev) RPYB_CUDA(cudaEventSynchronize(st.ev));   // its previous copy is done
+    if (st.cap < bytes) {
+        if (st.p) RPYB_CUDA(cudaFreeHost(st.p));
+        st.p = nullptr;
+        st.cap = 0;
+        const size_t cap = std::max<size_t>(bytes + bytes / 2, 1 << 20);
+        RPYB_CUDA(cudaMallocHost(&st.p, cap));
+        st.cap = cap;
+    }
+    if (!st.ev) RPYB_CUDA(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
+    std::memcpy(st.p, src, bytes);
+    RPYB_CUDA(cudaMemcpyAsync(dst, st.p, bytes, cudaMemcpyHostToDevice, s));
+    RPYB_CUDA(cudaEventRecord(st.ev, s));
     return RPYB_OK;
 }
 
@@ -166,8 +203,7 @@ int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, v
     if ((rc = sc.get(idx_bytes + 2 * buf, &mem))) return rc;
     int64_t* d_idx = static_cast<int64_t*>(mem);
     char* bufs[2] = {static_cast<char*>(mem) + idx_bytes, static_cast<char*>(mem) + idx_bytes + buf};
-    // the pageable source is read before cudaMemcpyAsync returns
-    RPYB_CUDA(cudaMemcpyAsync(d_idx, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice, s));
+    if ((rc = upload_async(d_idx, packed.data(), packed.size() * 8, s))) return rc;
     for (int64_t r = 0; r < maxc; ++r) {
         const int64_t m = active[r];
         const void* lhs = (r == 0) ? acc : bufs[(r - 1) & 1];
