@@ -163,7 +163,10 @@ RPYB_API int rpyb_piecewise_query(int32_t width, int32_t depth, int64_t n_pieces
             std::vector<int64_t> loff(m + 1), rows(nf);
             for (int64_t i = 0; i <= m; ++i) loff[i] = qoff[q0 + i] - f0;
             for (int64_t i = 0; i < nf; ++i) rows[i] = i;
-            if ((rc = ordered_products(RPYB_F64, RPYB_F64, g, m, acc, ex, loff, rows, s))) return rc;
+            if ((rc = chain_products_available(g)
+                          ? chain_products(RPYB_F64, g, m, acc, ex, loff, rows, s)
+                          : ordered_products(RPYB_F64, RPYB_F64, g, m, acc, ex, loff, rows, s)))
+                return rc;
         }
         if ((rc = finish_queries(g, *maps, m, acc, out_logsig ? out_logsig + q0 * ld_logsig : nullptr,
                                  ld_logsig, out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig,

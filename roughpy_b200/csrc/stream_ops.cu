@@ -112,7 +112,193 @@ int upload_async(void* dst, const void* src, size_t bytes, cudaStream_t s)
     return RPYB_OK;
 }
 
+
+// ------------------------------------------------------------------------
+// Fused chain products: one block per row q keeps acc[q] in shared memory
+// (float64, double-buffered) and multiplies in the rows src[r] of its list
+// one after the other, so the accumulator crosses HBM once instead of once
+// per factor.  A product is split like the blocked product kernel: a unit
+// owns D first letters x V last letters of one middle part at a level
+// k >= 2; levels 0 and 1 are done by the first threads.
+struct ChainArgs {
+    int64_t T = 0;
+    int64_t db[kMaxDepth + 2] = {};
+    int64_t pw[kMaxDepth + 1] = {};
+    int64_t ucum[kMaxDepth + 2] = {};   // work units before level k (k >= 2)
+    int64_t utotal = 0;
+    int depth = 0;
+    int64_t n = 0;
+    const int64_t* off = nullptr;      // [n + 1] into rows
+    const int64_t* rows = nullptr;     // source row of each factor
+    const void* src = nullptr;         // [*, T] factors (float or double)
+    double* acc = nullptr;             // [n, T] in/out
+};
+
+constexpr int kChainThreads = 512;
+
+template <typename TS, int D, int V>
+__global__ void __launch_bounds__(kChainThreads, 1)
+chain_products_kernel(const ChainArgs a)
+{
+    constexpr int NB = D / V;
+    extern __shared__ __align__(16) unsigned char chain_smem[];
+    double* buf0 = reinterpret_cast<double*>(chain_smem);
+    double* buf1 = buf0 + a.T;
+    const int tid = (int)threadIdx.x;
+    const TS* src = static_cast<const TS*>(a.src);
+    for (int64_t q = blockIdx.x; q < a.n; q += gridDim.x) {
+        const int64_t o0 = a.off[q], o1 = a.off[q + 1];
+        if (o0 == o1) continue;
+        double* accq = a.acc + q * a.T;
+        double* cur = buf0;
+        double* nxt = buf1;
+        __syncthreads();
+        for (int64_t i = tid; i < a.T; i += blockDim.x) cur[i] = accq[i];
+        __syncthreads();
+        for (int64_t r = o0; r < o1; ++r) {
+            const TS* node = src + a.rows[r] * a.T;
+            const double node0 = (double)__ldg(node);
+            const double c0v = cur[0];
+            if (tid == 0) nxt[0] = c0v * node0;
+            if (tid < D) nxt[1 + tid] = cur[1 + tid] * node0 + c0v * (double)__ldg(node + 1 + tid);
+            for (int64_t f = tid; f < a.utotal; f += blockDim.x) {
+                int k = 2;
+                while (f >= a.ucum[k + 1]) ++k;
+                const int64_t unit = f - a.ucum[k];
+                const uint32_t rp = (uint32_t)(unit / NB);
+                const int c0 = (int)(unit - (int64_t)rp * NB) * V;
+                const int64_t dk1 = a.pw[k - 1];
+                const int64_t obase = a.db[k] + (int64_t)rp * D + c0;
+                double acc[D][V];
+#pragma unroll
+                for (int u = 0; u < D; ++u)
+#pragma unroll
+                    for (int j = 0; j < V; ++j) acc[u][j] = cur[obase + u * dk1 + j] * node0;
+                uint32_t qq = rp;
+                uint32_t m = 0;
+                for (int s = 1; s <= k - 1; ++s) {
+                    const int p = k - s;
+                    double lv[D];
+                    double rv[V];
+                    const double* lp = cur + a.db[p] + qq;
+                    const uint32_t dp1 = (uint32_t)a.pw[p - 1];
+#pragma unroll
+                    for (int u = 0; u < D; ++u) lv[u] = lp[u * dp1];
+                    const TS* rq = node + a.db[s] + (int64_t)m * D + c0;
+#pragma unroll
+                    for (int j = 0; j < V; ++j) rv[j] = (double)__ldg(rq + j);
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j) acc[u][j] = fma(lv[u], rv[j], acc[u][j]);
+                    const uint32_t q2 = qq / (uint32_t)D;
+                    m += (qq - q2 * (uint32_t)D) * (uint32_t)a.pw[s - 1];
+                    qq = q2;
+                }
+#pragma unroll
+                for (int u = 0; u < D; ++u)
+#pragma unroll
+                    for (int j = 0; j < V; ++j)
+                        nxt[obase + u * dk1 + j] =
+                            fma(c0v, (double)__ldg(node + obase + u * dk1 + j), acc[u][j]);
+            }
+            __syncthreads();
+            double* t = cur;
+            cur = nxt;
+            nxt = t;
+        }
+        for (int64_t i = tid; i < a.T; i += blockDim.x) accq[i] = cur[i];
+    }
+}
+
+// width -> last-letter block of the chain kernel (0: not available)
+int chain_v(int width)
+{
+    switch (width) {
+        case 2: return 2;
+        case 3: return 3;
+        case 4: return 4;
+        case 5: return 5;
+        case 6: return 3;
+        case 8: return 2;
+        default: return 0;
+    }
+}
+
+template <typename TS>
+using ChainFn = void (*)(ChainArgs);
+
+template <typename TS>
+ChainFn<TS> chain_fn(int width)
+{
+    switch (width) {
+        case 2: return &chain_products_kernel<TS, 2, 2>;
+        case 3: return &chain_products_kernel<TS, 3, 3>;
+        case 4: return &chain_products_kernel<TS, 4, 4>;
+        case 5: return &chain_products_kernel<TS, 5, 5>;
+        case 6: return &chain_products_kernel<TS, 6, 3>;
+        case 8: return &chain_products_kernel<TS, 8, 2>;
+        default: return nullptr;
+    }
+}
+
+constexpr int64_t kChainSmemLimit = 200 * 1024;
+
 }  // namespace
+
+bool chain_products_available(const Geometry& g)
+{
+    return g.depth >= 2 && chain_v(g.width) > 0 && 2 * g.size() * 8 <= kChainSmemLimit;
+}
+
+int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
+                   const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                   cudaStream_t s)
+{
+    if (n == 0 || off[n] == 0) return RPYB_OK;
+    if (!chain_products_available(g)) return fail(RPYB_E_UNSUPPORTED, "no chain kernel for this shape");
+    const int V = chain_v(g.width);
+    ChainArgs a;
+    a.T = g.size();
+    for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
+    for (int k = 0; k <= kMaxDepth; ++k) a.pw[k] = g.pw[k];
+    int64_t u = 0;
+    for (int k = 0; k <= kMaxDepth + 1; ++k) a.ucum[k] = 0;
+    for (int k = 2; k <= g.depth; ++k) {
+        a.ucum[k] = u;
+        u += g.pw[k - 2] * (g.width / V);
+    }
+    for (int k = g.depth + 1; k <= kMaxDepth + 1; ++k) a.ucum[k] = u;
+    a.utotal = u;
+    a.depth = g.depth;
+    a.n = n;
+    // offsets and rows in one upload
+    std::vector<int64_t> packed(off.begin(), off.begin() + n + 1);
+    packed.insert(packed.end(), src_rows.begin(), src_rows.begin() + off[n]);
+    Scratch sc(nullptr, 0, s);
+    void* mem = nullptr;
+    int rc;
+    if ((rc = sc.get(packed.size() * 8, &mem))) return rc;
+    int64_t* d = static_cast<int64_t*>(mem);
+    if ((rc = upload_async(d, packed.data(), packed.size() * 8, s))) return rc;
+    a.off = d;
+    a.rows = d + n + 1;
+    a.src = src;
+    a.acc = acc;
+    const size_t smem = (size_t)(2 * a.T * 8);
+    const unsigned grid = (unsigned)std::min<int64_t>(n, 1 << 20);
+    if (src_mode == RPYB_F64) {
+        auto fn = chain_fn<double>(g.width);
+        RPYB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        fn<<<grid, kChainThreads, smem, s>>>(a);
+    } else {
+        auto fn = chain_fn<float>(g.width);
+        RPYB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        fn<<<grid, kChainThreads, smem, s>>>(a);
+    }
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
 
 int lie_maps_device(const Geometry& g, const LieMapsDev** out)
 {

@@ -38,6 +38,14 @@ int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, v
                      const void* src, const std::vector<int64_t>& off,
                      const std::vector<int64_t>& src_rows, cudaStream_t s);
 
+// Same as ordered_products for a float64 accumulator, fused: one block per
+// row keeps acc[q] in shared memory across its whole list of factors.
+// Available for widths 2..6 and 8 with 2 * tensor_size * 8 <= 200 KB.
+bool chain_products_available(const Geometry& g);
+int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
+                   const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                   cudaStream_t s);
+
 // Bytes of scratch finish_queries needs for up to `n` rows.
 size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n);
 
