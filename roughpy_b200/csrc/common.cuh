@@ -96,4 +96,12 @@ __device__ __forceinline__ void df_add_prod(DF& acc, float a, float b)
 
 __device__ __forceinline__ float df_value(const DF& a) { return __fadd_rn(a.hi, a.lo); }
 
+// Most pieces the dissection of one interval can produce.
+constexpr int kMaxDyadicPieces = 2 * (4 * 64 + 1);
+
+// Dissects the clopen interval [inf, sup) at resolution tol into maximal
+// dyadic pieces k / 2^p, in order; writes at most kMaxDyadicPieces and returns
+// their number, or a negative error code for an invalid interval or resolution.
+int dissect_clopen(double inf, double sup, int32_t tol, int64_t* k, int32_t* p);
+
 }  // namespace rpyb

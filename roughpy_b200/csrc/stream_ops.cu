@@ -473,55 +473,33 @@ int refine_and_dissect(int64_t n, const double* inf, const double* sup, double s
     const bool auto_res = resolution == RPYB_QUERY_RESOLUTION_AUTO;
     if (!auto_res && (resolution < -60 || resolution > 60))
         return fail(RPYB_E_INVALID, "query resolution out of range");
-    std::vector<double> qi(n), qs(n);
-    std::vector<int32_t> tol(n);
-    std::vector<char> empty(n, 0);
-    int32_t max_tol = 0;
+    k.clear();
+    p.clear();
+    k.reserve((size_t)n * 16);
+    p.reserve((size_t)n * 16);
+    poff.assign(n + 1, 0);
+    int64_t kb[kMaxDyadicPieces];
+    int32_t pb[kMaxDyadicPieces];
     for (int64_t q = 0; q < n; ++q) {
         double a = inf[q], b = sup[q];
         if (!(a <= b)) return fail(RPYB_E_INVALID, "inf must not be larger than sup");
-        if (b < s0 || a > s1) {
-            empty[q] = 1;
-            a = b = s0;
-        } else {
+        // trimmed to the support; empty queries keep no pieces
+        const bool outside = b < s0 || a > s1;
+        if (!outside) {
             a = std::max(a, s0);
             b = std::min(b, s1);
         }
-        if (b - a == 0.0) empty[q] = 1;
-        qi[q] = a;
-        qs[q] = b;
-        if (auto_res)
-            tol[q] = empty[q] ? default_resolution
-                              : std::max<int32_t>(default_resolution,
-                                                  query_param_to_resolution(b - a) + 2);
-        else
-            tol[q] = resolution;
-        max_tol = std::max(max_tol, std::abs(tol[q]));
+        if (!outside && b - a != 0.0) {
+            const int32_t tol =
+                auto_res ? std::max<int32_t>(default_resolution, query_param_to_resolution(b - a) + 2)
+                         : resolution;
+            const int np = dissect_clopen(a, b, tol, kb, pb);
+            if (np < 0) return np;
+            k.insert(k.end(), kb, kb + np);
+            p.insert(p.end(), pb, pb + np);
+        }
+        poff[q + 1] = (int64_t)k.size();
     }
-    const int64_t cap = std::max<int64_t>(1, n * (2 * (int64_t)max_tol + 130));
-    k.assign(cap, 0);
-    p.assign(cap, 0);
-    poff.assign(n + 1, 0);
-    int rc;
-    if ((rc = rpyb_dyadic_dissect_batch(n, qi.data(), qs.data(), tol.data(), 1, k.data(), p.data(),
-                                        cap, poff.data())))
-        return rc;
-    // empty queries keep no pieces
-    std::vector<int64_t> k2, off2(n + 1, 0);
-    std::vector<int32_t> p2;
-    k2.reserve(poff[n]);
-    p2.reserve(poff[n]);
-    for (int64_t q = 0; q < n; ++q) {
-        if (!empty[q])
-            for (int64_t i = poff[q]; i < poff[q + 1]; ++i) {
-                k2.push_back(k[i]);
-                p2.push_back(p[i]);
-            }
-        off2[q + 1] = (int64_t)k2.size();
-    }
-    k.swap(k2);
-    p.swap(p2);
-    poff.swap(off2);
     return RPYB_OK;
 }
 

@@ -56,6 +56,40 @@ def test_dissection_library_matches_restatement_and_tiles_the_interval():
         assert pos == hi or (not pieces and lo == hi)
 
 
+def test_dissection_walks_match_restatement_over_scales():
+    """Both of the library's walks (multipliers below 2^52, and the general one
+    between 2^52 and 2^53) against the restatement, over negative and large
+    resolutions and interval scales; the batched entry agrees with the single
+    one."""
+    rng = np.random.default_rng(12)
+    cases = []
+    for _ in range(3000):
+        tol = int(rng.integers(-8, 46))
+        top = min(20.0, 58.0 - max(tol, 0))
+        scale = 2.0 ** float(rng.uniform(-6.0, top))
+        a, b = np.sort(rng.uniform(-scale, scale, size=2))
+        cases.append((float(a), float(b), tol))
+    for _ in range(300):
+        sign = 1.0 if rng.random() < 0.5 else -1.0
+        a = sign * float(rng.uniform(4.0, 7.9))
+        cases.append((min(a, a + 0.05), max(a, a + 0.05), 50))
+    for a, b, tol in cases:
+        assert lib_dissect(a, b, tol) == R.to_dyadic_intervals(a, b, tol), (a, b, tol)
+    infs = np.array([c[0] for c in cases])
+    sups = np.array([c[1] for c in cases])
+    tols = np.array([c[2] for c in cases], dtype=np.int32)
+    cap = 200 * len(cases)
+    k = np.zeros(cap, np.int64)
+    p = np.zeros(cap, np.int32)
+    off = np.zeros(len(cases) + 1, np.int64)
+    assert _lib.lib.rpyb_dyadic_dissect_batch(len(cases), infs.ctypes.data, sups.ctypes.data,
+                                              tols.ctypes.data, 1, k.ctypes.data, p.ctypes.data,
+                                              cap, off.ctypes.data) == 0
+    for i, (a, b, tol) in enumerate(cases[:500]):
+        got = [(int(k[j]), int(p[j])) for j in range(off[i], off[i + 1])]
+        assert got == lib_dissect(a, b, tol)
+
+
 def test_batched_dissection_and_errors():
     infs = np.array([0.0, -1.0, 0.5])
     sups = np.array([1.63451, 1.25, 0.5])
