@@ -589,6 +589,25 @@ def profile_slice(n):
     print("profile slice done", n)
 
 
+def profile_queries(nq):
+    """The dyadic-query workload's tree (2^16 events, width 6, depth 5,
+    resolution 16, float32 nodes) and one query call of nq log-signatures: one
+    fused chain-product-and-log pass and one Hall projection per chunk of 8192
+    queries."""
+    import torch
+    from roughpy_b200.streams import LieIncrementStream
+    n = 1 << 16
+    rng = np.random.default_rng(3)
+    inc = rng.normal(0, np.sqrt(1.0 / n), size=(n, 6)).astype(np.float32)
+    idx = np.arange(n) / n
+    q = np.sort(np.floor(rng.uniform(0, 1, size=(nq, 2)) * n) / n, axis=1)
+    st = LieIncrementStream.from_increments(inc, indices=idx, width=6, depth=5, resolution=16)
+    st._build_tree()
+    st.log_signature_batch(q[:, 0], q[:, 1])
+    torch.cuda.synchronize()
+    print("profile queries done", nq)
+
+
 def profile_fma(w, d, batch):
     """One float64 and one float32 C += A (x) B launch over `batch` pairs."""
     import torch
@@ -691,6 +710,8 @@ def main():
                     help="run one launch per mode on an N-stream slice and exit")
     ap.add_argument("--profile-fma", type=int, nargs=3, metavar=("WIDTH", "DEPTH", "BATCH"),
                     help="run one float64 and one float32 FMA launch and exit")
+    ap.add_argument("--profile-queries", type=int, default=0,
+                    help="build the dyadic-query tree, run N queries and exit")
     args = ap.parse_args()
     if args.profile_backward:
         profile_backward(args.profile_backward)
@@ -700,6 +721,9 @@ def main():
         return
     if args.profile_fma:
         profile_fma(*args.profile_fma)
+        return
+    if args.profile_queries:
+        profile_queries(args.profile_queries)
         return
     if args.warmup < 3 and args.impl == "b200":
         log("note: warmup raised to 3")

@@ -293,7 +293,7 @@ RPYB_API int64_t rpyb_lie_map_csr(int32_t width, int32_t depth, int which,
  * y[b] += scale * M x[b] for a CSR matrix M (device arrays, float64 values),
  * batched over rows; x, y of dtype (float32 rows are computed in float64).
  * The map accumulates into y, as the reference's does: zero y for a plain
- * product.
+ * product.  Entries whose column index lies outside [0, n_cols) are skipped.
  * Replaces: roughpy_compute/dense/basic/apply_sparse_linear_map.hpp:16-55 via
  *           roughpy/compute/_src/dense_basic.cpp:564-620 and :1055-1150.
  */

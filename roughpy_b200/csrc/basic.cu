@@ -83,9 +83,11 @@ __global__ void adjoint_left_mul_kernel(T* out, const T* op, const T* arg, int64
     }
 }
 
-// y[b][r] += scale * sum_k val[k] * x[b][idx[k]]  (CSR), float64 accumulation.
+// y[b][r] += scale * sum_k val[k] * x[b][idx[k]]  (CSR), float64 accumulation;
+// column indices outside [0, n_cols) are skipped.
 template <typename T>
-__global__ void csr_map_kernel(int64_t n_rows, int64_t batch, const int64_t* __restrict__ ptr,
+__global__ void csr_map_kernel(int64_t n_rows, int64_t n_cols, int64_t batch,
+                               const int64_t* __restrict__ ptr,
                                const int64_t* __restrict__ idx, const double* __restrict__ val,
                                T* y, const T* x, int64_t ld_y, int64_t ld_x, double scale)
 {
@@ -96,8 +98,10 @@ __global__ void csr_map_kernel(int64_t n_rows, int64_t batch, const int64_t* __r
         const int64_t r = g - b * n_rows;
         const T* xr = x + b * ld_x;
         double acc = 0.0;
-        for (int64_t k = __ldg(ptr + r), e = __ldg(ptr + r + 1); k < e; ++k)
-            acc = fma(__ldg(val + k), (double)__ldg(xr + __ldg(idx + k)), acc);
+        for (int64_t k = __ldg(ptr + r), e = __ldg(ptr + r + 1); k < e; ++k) {
+            const int64_t c = __ldg(idx + k);
+            if ((uint64_t)c < (uint64_t)n_cols) acc = fma(__ldg(val + k), (double)__ldg(xr + c), acc);
+        }
         T* yp = y + b * ld_y + r;
         *yp = (T)((double)*yp + scale * acc);
     }
@@ -207,12 +211,12 @@ RPYB_API int rpyb_sparse_map(int dtype, int64_t n_rows, int64_t n_cols, int64_t 
     const int threads = 256;
     const unsigned blocks = grid_for(n_rows * batch, threads);
     if (dtype == RPYB_F64)
-        csr_map_kernel<double><<<blocks, threads, 0, s>>>(n_rows, batch, indptr, indices, values,
+        csr_map_kernel<double><<<blocks, threads, 0, s>>>(n_rows, n_cols, batch, indptr, indices, values,
                                                          static_cast<double*>(y),
                                                          static_cast<const double*>(x), ld_y,
                                                          ld_x, scale);
     else
-        csr_map_kernel<float><<<blocks, threads, 0, s>>>(n_rows, batch, indptr, indices, values,
+        csr_map_kernel<float><<<blocks, threads, 0, s>>>(n_rows, n_cols, batch, indptr, indices, values,
                                                         static_cast<float*>(y),
                                                         static_cast<const float*>(x), ld_y, ld_x,
                                                         scale);

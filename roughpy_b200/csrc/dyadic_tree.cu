@@ -346,11 +346,12 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* t, int64_t n_queries,
             }
             qoff[q + 1] = (int64_t)nodes.size();
         }
-        if ((rc = unit_rows(RPYB_F64, acc, T, T, nullptr, m, s)) ||
-            (rc = chain_products_available(g)
-                      ? chain_products(t->mode, g, m, acc, t->nodes, qoff, nodes, s)
-                      : ordered_products(RPYB_F64, t->mode, g, m, acc, t->nodes, qoff, nodes, s)) ||
-            (rc = finish_queries(g, *t->maps, m, acc,
+        const bool chain = chain_products_available(g);
+        if ((rc = chain ? chain_products(t->mode, g, m, acc, t->nodes, qoff, nodes, true, s)
+                        : (unit_rows(RPYB_F64, acc, T, T, nullptr, m, s) ||
+                           ordered_products(RPYB_F64, t->mode, g, m, acc, t->nodes, qoff, nodes,
+                                            s))) ||
+            (rc = finish_queries(g, *t->maps, m, acc, chain,
                                  out_logsig ? out_logsig + q0 * ld_logsig : nullptr, ld_logsig,
                                  out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig, fin_mem, fin,
                                  s)))

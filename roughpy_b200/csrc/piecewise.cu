@@ -142,7 +142,8 @@ RPYB_API int rpyb_piecewise_query(int32_t width, int32_t depth, int64_t n_pieces
     for (size_t c = 0; c + 1 < starts.size(); ++c) {
         const int64_t q0 = starts[c], q1 = starts[c + 1], m = q1 - q0;
         const int64_t f0 = qoff[q0], nf = qoff[q1] - f0;
-        if ((rc = unit_rows(RPYB_F64, acc, T, T, nullptr, m, s))) return rc;
+        const bool chain = chain_products_available(g) && nf > 0;
+        if (!chain && (rc = unit_rows(RPYB_F64, acc, T, T, nullptr, m, s))) return rc;
         if (nf > 0) {
             RPYB_CUDA(cudaMemcpyAsync(d_piece, fpiece.data() + f0, (size_t)nf * 8,
                                       cudaMemcpyHostToDevice, s));
@@ -163,12 +164,12 @@ RPYB_API int rpyb_piecewise_query(int32_t width, int32_t depth, int64_t n_pieces
             std::vector<int64_t> loff(m + 1), rows(nf);
             for (int64_t i = 0; i <= m; ++i) loff[i] = qoff[q0 + i] - f0;
             for (int64_t i = 0; i < nf; ++i) rows[i] = i;
-            if ((rc = chain_products_available(g)
-                          ? chain_products(RPYB_F64, g, m, acc, ex, loff, rows, s)
-                          : ordered_products(RPYB_F64, RPYB_F64, g, m, acc, ex, loff, rows, s)))
+            if ((rc = chain ? chain_products(RPYB_F64, g, m, acc, ex, loff, rows, true, s)
+                            : ordered_products(RPYB_F64, RPYB_F64, g, m, acc, ex, loff, rows, s)))
                 return rc;
         }
-        if ((rc = finish_queries(g, *maps, m, acc, out_logsig ? out_logsig + q0 * ld_logsig : nullptr,
+        if ((rc = finish_queries(g, *maps, m, acc, chain,
+                                 out_logsig ? out_logsig + q0 * ld_logsig : nullptr,
                                  ld_logsig, out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig,
                                  fin_mem, fin_b, s)))
             return rc;

@@ -1,5 +1,6 @@
 // Shared stream building blocks (see stream_ops.cuh).
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -52,8 +53,44 @@ int32_t query_param_to_resolution(double length)
     return -std::min(0, e - 1);
 }
 
+template <typename E>
+int upload(const std::vector<E>& h, const E** out)
+{
+    E* d = nullptr;
+    RPYB_CUDA(cudaMalloc(&d, std::max<size_t>(h.size(), 1) * sizeof(E)));
+    if (!h.empty()) RPYB_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(E), cudaMemcpyHostToDevice));
+    *out = d;
+    return RPYB_OK;
+}
+
+// the packed form of a CSR map (column | value id << 16 per entry); false
+// when a column or the number of distinct values does not fit 16 bits
+bool pack_csr(const std::vector<int64_t>& hp, const std::vector<int64_t>& hi,
+              const std::vector<double>& hv, int64_t nnz, int64_t n_cols,
+              std::vector<uint32_t>& pptr, std::vector<uint32_t>& ent, std::vector<double>& tab)
+{
+    if (nnz >= ((int64_t)1 << 32) || n_cols > 0x10000) return false;
+    std::map<uint64_t, uint32_t> ids;   // keyed by the value's bits
+    pptr.assign(hp.begin(), hp.end());
+    ent.resize((size_t)nnz);
+    tab.clear();
+    for (int64_t k = 0; k < nnz; ++k) {
+        if (hi[k] < 0 || hi[k] >= n_cols) return false;
+        uint64_t bits;
+        std::memcpy(&bits, &hv[k], sizeof bits);
+        auto it = ids.find(bits);
+        if (it == ids.end()) {
+            if (tab.size() > 0xffff) return false;
+            it = ids.emplace(bits, (uint32_t)tab.size()).first;
+            tab.push_back(hv[k]);
+        }
+        ent[k] = (uint32_t)hi[k] | (it->second << 16);
+    }
+    return true;
+}
+
 int upload_csr(const Geometry& g, int which, int64_t n_rows, const int64_t** ptr,
-               const int64_t** idx, const double** val)
+               const int64_t** idx, const double** val, LieMapsDev* packed_into = nullptr)
 {
     const int64_t nnz = rpyb_lie_map_csr(g.width, g.depth, which, nullptr, nullptr, nullptr);
     if (nnz < 0) return (int)nnz;
@@ -61,6 +98,19 @@ int upload_csr(const Geometry& g, int which, int64_t n_rows, const int64_t** ptr
     std::vector<double> hv(std::max<int64_t>(nnz, 1));
     const int64_t got = rpyb_lie_map_csr(g.width, g.depth, which, hp.data(), hi.data(), hv.data());
     if (got < 0) return (int)got;
+    if (packed_into) {
+        std::vector<uint32_t> pptr, ent;
+        std::vector<double> tab;
+        if (pack_csr(hp, hi, hv, nnz, g.size(), pptr, ent, tab)) {
+            int rc;
+            if ((rc = upload(pptr, &packed_into->t2l_pptr)) ||
+                (rc = upload(ent, &packed_into->t2l_ent)) ||
+                (rc = upload(tab, &packed_into->t2l_tab)))
+                return rc;
+            packed_into->t2l_nnz = nnz;
+            packed_into->t2l_ntab = (int64_t)tab.size();
+        }
+    }
     int64_t* dp = nullptr;
     int64_t* di = nullptr;
     double* dv = nullptr;
@@ -114,87 +164,268 @@ int upload_async(void* dst, const void* src, size_t bytes, cudaStream_t s)
 
 
 // ------------------------------------------------------------------------
-// Fused chain products: one block per row q keeps acc[q] in shared memory
-// (float64, double-buffered) and multiplies in the rows src[r] of its list
-// one after the other, so the accumulator crosses HBM once instead of once
-// per factor.  A product is split like the blocked product kernel: a unit
-// owns D first letters x V last letters of one middle part at a level
-// k >= 2; levels 0 and 1 are done by the first threads.
+// Tensor -> Lie projection with the packed map held in shared memory.  One
+// persistent block per SM loads the map (column and value id per entry, the
+// distinct values, the row pointers) once; for each of its rows of x it
+// copies the row into shared memory with coalesced loads and computes every
+// Lie coordinate from shared memory.  The compact entries are what makes
+// this pay: as (int64, float64) pairs the map is larger than a row of x and
+// its gathers go to L2 for every row.
+constexpr int kProjThreads = 1024;
+constexpr int64_t kProjSmemLimit = 220 * 1024;
+
+struct ProjArgs {
+    int64_t n_rows = 0, n_cols = 0, nnz = 0, ntab = 0, batch = 0;
+    int64_t ld_y = 0, ld_x = 0;
+    const uint32_t* pptr = nullptr;
+    const uint32_t* ent = nullptr;
+    const double* tab = nullptr;
+};
+
+template <typename T>
+size_t proj_smem_bytes(const ProjArgs& a)
+{
+    return (size_t)(a.ntab * 8 + a.n_cols * (int64_t)sizeof(T) + (a.n_rows + 1) * 4 + a.nnz * 4);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kProjThreads, 1)
+lie_project_kernel(const ProjArgs a, T* __restrict__ y, const T* __restrict__ x)
+{
+    extern __shared__ __align__(16) unsigned char proj_smem[];
+    double* tab = reinterpret_cast<double*>(proj_smem);
+    T* xs = reinterpret_cast<T*>(tab + a.ntab);
+    uint32_t* pptr = reinterpret_cast<uint32_t*>(xs + a.n_cols);
+    uint32_t* ent = pptr + a.n_rows + 1;
+    const int tid = (int)threadIdx.x;
+    for (int64_t i = tid; i < a.ntab; i += blockDim.x) tab[i] = a.tab[i];
+    for (int64_t i = tid; i <= a.n_rows; i += blockDim.x) pptr[i] = a.pptr[i];
+    for (int64_t i = tid; i < a.nnz; i += blockDim.x) ent[i] = a.ent[i];
+    constexpr int kU = 8;
+    for (int64_t b = blockIdx.x; b < a.batch; b += gridDim.x) {
+        __syncthreads();   // the map is loaded; the previous row's gathers are done
+        const T* xr = x + b * a.ld_x;
+        // eight independent loads in flight per thread
+        for (int64_t c0 = tid; c0 < a.n_cols; c0 += kU * blockDim.x) {
+            T v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int64_t c = c0 + (int64_t)u * blockDim.x;
+                v[u] = c < a.n_cols ? __ldg(xr + c) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int64_t c = c0 + (int64_t)u * blockDim.x;
+                if (c < a.n_cols) xs[c] = v[u];
+            }
+        }
+        __syncthreads();
+        if (b + gridDim.x < a.batch) {
+            // the block's next row into L2 while this one is computed
+            const char* nx = reinterpret_cast<const char*>(x + (b + gridDim.x) * a.ld_x);
+            const int64_t bytes = a.n_cols * (int64_t)sizeof(T);
+            for (int64_t l = (int64_t)tid * 128; l < bytes; l += (int64_t)blockDim.x * 128)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + l));
+        }
+        T* yr = y + b * a.ld_y;
+        for (int64_t r = tid; r < a.n_rows; r += blockDim.x) {
+            double acc = 0.0;
+            const uint32_t e = pptr[r + 1];
+            for (uint32_t k = pptr[r]; k < e; ++k) {
+                const uint32_t w = ent[k];
+                acc = fma(tab[w >> 16], (double)xs[w & 0xffffu], acc);
+            }
+            yr[r] = (T)acc;
+        }
+    }
+}
+
+template <typename T>
+int launch_lie_project(const ProjArgs& a, void* y, const void* x, cudaStream_t s)
+{
+    const size_t smem = proj_smem_bytes<T>(a);
+    RPYB_CUDA(cudaFuncSetAttribute(lie_project_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    const unsigned blocks = (unsigned)std::min<int64_t>(a.batch, 148);
+    lie_project_kernel<T><<<blocks, kProjThreads, smem, s>>>(a, static_cast<T*>(y),
+                                                             static_cast<const T*>(x));
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
+// ------------------------------------------------------------------------
+// Fused chain products: acc[q] <- src[r_0] * src[r_1] * ... (the unit for an
+// empty list), or its float64 log, one block per row q, so that the running
+// product never leaves the SM.  Its levels below the top are in shared
+// memory (float64, double-buffered); its top level is spread over the
+// threads' registers.  That split is exact: a top-level output word reads
+// the lower levels of the left operand, the factor's words and only its own
+// top-level word of the left operand (times the factor's scalar), so no
+// thread needs another thread's top-level words.  A product is split like
+// the blocked product kernel: a unit owns D first letters x V last letters
+// of one middle part at a level k >= 2; levels 0 and 1 are done by the first
+// threads.  Every thread owns TU top-level units (flat units tid, tid + B,
+// ...); the lower units follow in the same flat order from the level below
+// the top down, so the threads that take one more unit take a light one.
+// The first factor is copied, not multiplied by the unit.  Factors are read
+// from global memory (queries share them, so the popular ones stay in L2),
+// and the next one is prefetched into L2 while a product runs.
 struct ChainArgs {
     int64_t T = 0;
     int64_t db[kMaxDepth + 2] = {};
     int64_t pw[kMaxDepth + 1] = {};
-    int64_t ucum[kMaxDepth + 2] = {};   // work units before level k (k >= 2)
-    int64_t utotal = 0;
+    int64_t lo_begin[kMaxDepth + 2] = {};   // first lower unit of level k (2 <= k < depth)
+    int64_t utop = 0, ulow = 0;             // top-level and lower units
     int depth = 0;
     int64_t n = 0;
     const int64_t* off = nullptr;      // [n + 1] into rows
     const int64_t* rows = nullptr;     // source row of each factor
     const void* src = nullptr;         // [*, T] factors (float or double)
-    double* acc = nullptr;             // [n, T] in/out
+    double* acc = nullptr;             // [n, T] out
+    int log_out = 0;                   // write log(product) instead of the product
 };
 
 constexpr int kChainThreads = 512;
 
-template <typename TS, int D, int V>
+// out[D][V] (+)= sum over s = 1..k-1 of lhs level k-s (x) rhs level s at the
+// unit (rp, c0) of level k: the left factor's D words of first letters u at
+// middle part rp's prefix, the right factor's V words after it
+template <int D, int V, typename TR, bool GLOBAL_RHS>
+__device__ __forceinline__ void unit_splits(double (&acc)[D][V], const double* lhs, const TR* rhs,
+                                            const ChainArgs& a, int k, uint32_t rp, int c0)
+{
+    uint32_t qq = rp;
+    uint32_t m = 0;
+    for (int s = 1; s <= k - 1; ++s) {
+        const int p = k - s;
+        double lv[D];
+        double rv[V];
+        const double* lp = lhs + a.db[p] + qq;
+        const uint32_t dp1 = (uint32_t)a.pw[p - 1];
+#pragma unroll
+        for (int u = 0; u < D; ++u) lv[u] = lp[u * dp1];
+        const TR* rq = rhs + a.db[s] + (int64_t)m * D + c0;
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            if constexpr (GLOBAL_RHS) rv[j] = (double)__ldg(rq + j);
+            else rv[j] = (double)rq[j];
+        }
+#pragma unroll
+        for (int u = 0; u < D; ++u)
+#pragma unroll
+            for (int j = 0; j < V; ++j) acc[u][j] = fma(lv[u], rv[j], acc[u][j]);
+        const uint32_t q2 = qq / (uint32_t)D;
+        m += (qq - q2 * (uint32_t)D) * (uint32_t)a.pw[s - 1];
+        qq = q2;
+    }
+}
+
+// the level and position of lower unit li (levels depth-1 down to 2)
+template <int D, int V>
+__device__ __forceinline__ void lower_unit(const ChainArgs& a, int64_t li, int& k, uint32_t& rp,
+                                           int& c0, int64_t& obase, int64_t& dk1)
+{
+    constexpr int NB = D / V;
+    k = a.depth - 1;
+    while (k > 2 && li >= a.lo_begin[k - 1]) --k;
+    const int64_t unit = li - a.lo_begin[k];
+    rp = (uint32_t)(unit / NB);
+    c0 = (int)(unit - (int64_t)rp * NB) * V;
+    dk1 = a.pw[k - 1];
+    obase = a.db[k] + (int64_t)rp * D + c0;
+}
+
+template <typename TS, int D, int V, int TU>
 __global__ void __launch_bounds__(kChainThreads, 1)
 chain_products_kernel(const ChainArgs a)
 {
     constexpr int NB = D / V;
     extern __shared__ __align__(16) unsigned char chain_smem[];
-    double* buf0 = reinterpret_cast<double*>(chain_smem);
-    double* buf1 = buf0 + a.T;
+    const int N = a.depth;
+    const int64_t TL = a.db[N];   // words below the top level
+    double* lo0 = reinterpret_cast<double*>(chain_smem);
+    double* lo1 = lo0 + TL;
     const int tid = (int)threadIdx.x;
+    const int B = (int)blockDim.x;
     const TS* src = static_cast<const TS*>(a.src);
+    const int64_t tdk1 = a.pw[N - 1];
+    // this thread's top-level units: output words tbase[t] + u * tdk1 + j
+    int64_t tbase[TU];
+    uint32_t trp[TU];
+    int tc0[TU];
+    bool town[TU];
+#pragma unroll
+    for (int t = 0; t < TU; ++t) {
+        const int64_t f = tid + (int64_t)t * B;
+        town[t] = f < a.utop;
+        trp[t] = town[t] ? (uint32_t)(f / NB) : 0u;
+        tc0[t] = town[t] ? (int)(f - (int64_t)trp[t] * NB) * V : 0;
+        tbase[t] = a.db[N] + (int64_t)trp[t] * D + tc0[t];
+    }
+    int64_t f_low = tid;   // this thread's first lower unit (flat index)
+    while (f_low < a.utop) f_low += B;
+
     for (int64_t q = blockIdx.x; q < a.n; q += gridDim.x) {
         const int64_t o0 = a.off[q], o1 = a.off[q + 1];
-        if (o0 == o1) continue;
         double* accq = a.acc + q * a.T;
-        double* cur = buf0;
-        double* nxt = buf1;
-        __syncthreads();
-        for (int64_t i = tid; i < a.T; i += blockDim.x) cur[i] = accq[i];
-        __syncthreads();
-        for (int64_t r = o0; r < o1; ++r) {
+        if (o0 == o1) {   // the unit, or its log
+            for (int64_t i = tid; i < a.T; i += B) accq[i] = (i == 0 && !a.log_out) ? 1.0 : 0.0;
+            continue;
+        }
+        double* cur = lo0;
+        double* nxt = lo1;
+        __syncthreads();   // the previous row's reads of the buffers are done
+        const TS* first = src + a.rows[o0] * a.T;
+        for (int64_t i = tid; i < TL; i += B) cur[i] = (double)__ldg(first + i);
+        double top[TU][D][V];
+#pragma unroll
+        for (int t = 0; t < TU; ++t)
+#pragma unroll
+            for (int u = 0; u < D; ++u)
+#pragma unroll
+                for (int j = 0; j < V; ++j)
+                    top[t][u][j] = town[t] ? (double)__ldg(first + tbase[t] + u * tdk1 + j) : 0.0;
+        for (int64_t r = o0 + 1; r < o1; ++r) {
+            __syncthreads();
             const TS* node = src + a.rows[r] * a.T;
+            if (r + 1 < o1) {
+                const char* nn = reinterpret_cast<const char*>(src + a.rows[r + 1] * a.T);
+                const int64_t bytes = a.T * (int64_t)sizeof(TS);
+                for (int64_t l = (int64_t)tid * 128; l < bytes; l += (int64_t)B * 128)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(nn + l));
+            }
             const double node0 = (double)__ldg(node);
             const double c0v = cur[0];
             if (tid == 0) nxt[0] = c0v * node0;
             if (tid < D) nxt[1 + tid] = cur[1 + tid] * node0 + c0v * (double)__ldg(node + 1 + tid);
-            for (int64_t f = tid; f < a.utotal; f += blockDim.x) {
-                int k = 2;
-                while (f >= a.ucum[k + 1]) ++k;
-                const int64_t unit = f - a.ucum[k];
-                const uint32_t rp = (uint32_t)(unit / NB);
-                const int c0 = (int)(unit - (int64_t)rp * NB) * V;
-                const int64_t dk1 = a.pw[k - 1];
-                const int64_t obase = a.db[k] + (int64_t)rp * D + c0;
+            // top-level units, in registers
+#pragma unroll
+            for (int t = 0; t < TU; ++t) {
+                if (!town[t]) continue;
+#pragma unroll
+                for (int u = 0; u < D; ++u)
+#pragma unroll
+                    for (int j = 0; j < V; ++j) top[t][u][j] *= node0;
+                unit_splits<D, V, TS, true>(top[t], cur, node, a, N, trp[t], tc0[t]);
+#pragma unroll
+                for (int u = 0; u < D; ++u)
+#pragma unroll
+                    for (int j = 0; j < V; ++j)
+                        top[t][u][j] =
+                            fma(c0v, (double)__ldg(node + tbase[t] + u * tdk1 + j), top[t][u][j]);
+            }
+            // lower units, in shared memory
+            for (int64_t f = f_low; f < a.utop + a.ulow; f += B) {
+                int k, c0;
+                uint32_t rp;
+                int64_t obase, dk1;
+                lower_unit<D, V>(a, f - a.utop, k, rp, c0, obase, dk1);
                 double acc[D][V];
 #pragma unroll
                 for (int u = 0; u < D; ++u)
 #pragma unroll
                     for (int j = 0; j < V; ++j) acc[u][j] = cur[obase + u * dk1 + j] * node0;
-                uint32_t qq = rp;
-                uint32_t m = 0;
-                for (int s = 1; s <= k - 1; ++s) {
-                    const int p = k - s;
-                    double lv[D];
-                    double rv[V];
-                    const double* lp = cur + a.db[p] + qq;
-                    const uint32_t dp1 = (uint32_t)a.pw[p - 1];
-#pragma unroll
-                    for (int u = 0; u < D; ++u) lv[u] = lp[u * dp1];
-                    const TS* rq = node + a.db[s] + (int64_t)m * D + c0;
-#pragma unroll
-                    for (int j = 0; j < V; ++j) rv[j] = (double)__ldg(rq + j);
-#pragma unroll
-                    for (int u = 0; u < D; ++u)
-#pragma unroll
-                        for (int j = 0; j < V; ++j) acc[u][j] = fma(lv[u], rv[j], acc[u][j]);
-                    const uint32_t q2 = qq / (uint32_t)D;
-                    m += (qq - q2 * (uint32_t)D) * (uint32_t)a.pw[s - 1];
-                    qq = q2;
-                }
+                unit_splits<D, V, TS, true>(acc, cur, node, a, k, rp, c0);
 #pragma unroll
                 for (int u = 0; u < D; ++u)
 #pragma unroll
@@ -207,7 +438,66 @@ chain_products_kernel(const ChainArgs a)
             cur = nxt;
             nxt = t;
         }
-        for (int64_t i = tid; i < a.T; i += blockDim.x) accq[i] = cur[i];
+        if (a.log_out) {
+            // log(X) of the product X by the Horner steps of the float64 log
+            // (free_tensor_log.hpp:23-38): with Y = X - X_0 and R = 0, for
+            // deg = N down to 1, R <- (R + c_deg) Y truncated to the levels
+            // N - deg + 1 and below, c_deg = (-1)^(deg+1) / deg.  Y's lower
+            // levels stay in `cur`, its top level in `top`; R's lower levels
+            // ping-pong between `nxt` and a third buffer.  R's top level is
+            // formed only in the last step, in place of Y's own top words.
+            double* rc = nxt;
+            double* rn = lo0 + 2 * TL;   // the third buffer
+            for (int s = 1; s <= N; ++s) {
+                const int deg = N - s + 1;
+                const double c = (deg % 2 == 0) ? -1.0 / (double)deg : 1.0 / (double)deg;
+                __syncthreads();   // R's previous step (and Y) complete
+                if (tid < D) rn[1 + tid] = c * cur[1 + tid];
+                if (s == N) {
+#pragma unroll
+                    for (int t = 0; t < TU; ++t) {
+                        if (!town[t]) continue;
+#pragma unroll
+                        for (int u = 0; u < D; ++u)
+#pragma unroll
+                            for (int j = 0; j < V; ++j) top[t][u][j] *= c;
+                        unit_splits<D, V, double, false>(top[t], rc, cur, a, N, trp[t], tc0[t]);
+                    }
+                }
+                for (int64_t f = f_low; f < a.utop + a.ulow; f += B) {
+                    int k, c0;
+                    uint32_t rp;
+                    int64_t obase, dk1;
+                    lower_unit<D, V>(a, f - a.utop, k, rp, c0, obase, dk1);
+                    if (k > s) continue;
+                    double acc[D][V];
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j) acc[u][j] = c * cur[obase + u * dk1 + j];
+                    unit_splits<D, V, double, false>(acc, rc, cur, a, k, rp, c0);
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j) rn[obase + u * dk1 + j] = acc[u][j];
+                }
+                double* t = rc;
+                rc = rn;
+                rn = t;
+            }
+            __syncthreads();
+            if (tid == 0) rc[0] = 0.0;
+            __syncthreads();
+            cur = rc;
+        }
+        for (int64_t i = tid; i < TL; i += B) accq[i] = cur[i];
+#pragma unroll
+        for (int t = 0; t < TU; ++t)
+            if (town[t])
+#pragma unroll
+                for (int u = 0; u < D; ++u)
+#pragma unroll
+                    for (int j = 0; j < V; ++j) accq[tbase[t] + u * tdk1 + j] = top[t][u][j];
     }
 }
 
@@ -218,26 +508,45 @@ int chain_v(int width)
         case 2: return 2;
         case 3: return 3;
         case 4: return 4;
-        case 5: return 5;
+        case 5: return 1;
         case 6: return 3;
         case 8: return 2;
         default: return 0;
     }
 }
 
-template <typename TS>
+// top-level units a thread holds in registers (0: the shape is not
+// covered); two only where two units' words fit the registers unspilled
+int chain_tu(const Geometry& g)
+{
+    const int V = chain_v(g.width);
+    if (V == 0 || g.depth < 2) return 0;
+    const int64_t utop = g.pw[g.depth - 2] * (g.width / V);
+    const int64_t tu = (utop + kChainThreads - 1) / kChainThreads;
+    if (tu == 1) return 1;
+    if (tu == 2 && g.width <= 3) return 2;
+    return 0;
+}
+
 using ChainFn = void (*)(ChainArgs);
 
 template <typename TS>
-ChainFn<TS> chain_fn(int width)
+ChainFn chain_fn(int width, int tu)
 {
+    if (tu == 2) {
+        switch (width) {
+            case 2: return &chain_products_kernel<TS, 2, 2, 2>;
+            case 3: return &chain_products_kernel<TS, 3, 3, 2>;
+            default: return nullptr;
+        }
+    }
     switch (width) {
-        case 2: return &chain_products_kernel<TS, 2, 2>;
-        case 3: return &chain_products_kernel<TS, 3, 3>;
-        case 4: return &chain_products_kernel<TS, 4, 4>;
-        case 5: return &chain_products_kernel<TS, 5, 5>;
-        case 6: return &chain_products_kernel<TS, 6, 3>;
-        case 8: return &chain_products_kernel<TS, 8, 2>;
+        case 2: return &chain_products_kernel<TS, 2, 2, 1>;
+        case 3: return &chain_products_kernel<TS, 3, 3, 1>;
+        case 4: return &chain_products_kernel<TS, 4, 4, 1>;
+        case 5: return &chain_products_kernel<TS, 5, 1, 1>;
+        case 6: return &chain_products_kernel<TS, 6, 3, 1>;
+        case 8: return &chain_products_kernel<TS, 8, 2, 1>;
         default: return nullptr;
     }
 }
@@ -248,28 +557,36 @@ constexpr int64_t kChainSmemLimit = 200 * 1024;
 
 bool chain_products_available(const Geometry& g)
 {
-    return g.depth >= 2 && chain_v(g.width) > 0 && 2 * g.size() * 8 <= kChainSmemLimit;
+    return chain_tu(g) > 0 && 3 * g.db[g.depth] * 8 <= kChainSmemLimit;
 }
 
 int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                    const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
-                   cudaStream_t s)
+                   bool log_out, cudaStream_t s)
 {
-    if (n == 0 || off[n] == 0) return RPYB_OK;
+    if (n == 0) return RPYB_OK;
     if (!chain_products_available(g)) return fail(RPYB_E_UNSUPPORTED, "no chain kernel for this shape");
-    const int V = chain_v(g.width);
+    if (off[n] == 0) {
+        if (log_out) {
+            RPYB_CUDA(cudaMemsetAsync(acc, 0, (size_t)(n * g.size() * 8), s));
+            return RPYB_OK;
+        }
+        return unit_rows(RPYB_F64, acc, g.size(), g.size(), nullptr, n, s);
+    }
+    const int V = chain_v(g.width), NB = g.width / V, tu = chain_tu(g);
     ChainArgs a;
     a.T = g.size();
     for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
     for (int k = 0; k <= kMaxDepth; ++k) a.pw[k] = g.pw[k];
+    a.utop = g.pw[g.depth - 2] * NB;
+    // lower levels depth-1 down to 2, in that order
     int64_t u = 0;
-    for (int k = 0; k <= kMaxDepth + 1; ++k) a.ucum[k] = 0;
-    for (int k = 2; k <= g.depth; ++k) {
-        a.ucum[k] = u;
-        u += g.pw[k - 2] * (g.width / V);
+    for (int k = g.depth - 1; k >= 2; --k) {
+        a.lo_begin[k] = u;
+        u += g.pw[k - 2] * NB;
     }
-    for (int k = g.depth + 1; k <= kMaxDepth + 1; ++k) a.ucum[k] = u;
-    a.utotal = u;
+    a.lo_begin[1] = u;
+    a.ulow = u;
     a.depth = g.depth;
     a.n = n;
     // offsets and rows in one upload
@@ -285,17 +602,13 @@ int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, cons
     a.rows = d + n + 1;
     a.src = src;
     a.acc = acc;
-    const size_t smem = (size_t)(2 * a.T * 8);
+    a.log_out = log_out ? 1 : 0;
+    const size_t smem = (size_t)((log_out ? 3 : 2) * g.db[g.depth] * 8);
     const unsigned grid = (unsigned)std::min<int64_t>(n, 1 << 20);
-    if (src_mode == RPYB_F64) {
-        auto fn = chain_fn<double>(g.width);
+    ChainFn fn = src_mode == RPYB_F64 ? chain_fn<double>(g.width, tu) : chain_fn<float>(g.width, tu);
+    if (smem > 48 * 1024)
         RPYB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        fn<<<grid, kChainThreads, smem, s>>>(a);
-    } else {
-        auto fn = chain_fn<float>(g.width);
-        RPYB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        fn<<<grid, kChainThreads, smem, s>>>(a);
-    }
+    fn<<<grid, kChainThreads, smem, s>>>(a);
     RPYB_CUDA(cudaGetLastError());
     return RPYB_OK;
 }
@@ -323,7 +636,7 @@ int lie_maps_device(const Geometry& g, const LieMapsDev** out)
     e.lie_dim = lie_dim;
     int rc;
     if ((rc = upload_csr(g, 0, g.size(), &e.l2t_ptr, &e.l2t_idx, &e.l2t_val)) ||
-        (rc = upload_csr(g, 1, lie_dim, &e.t2l_ptr, &e.t2l_idx, &e.t2l_val)))
+        (rc = upload_csr(g, 1, lie_dim, &e.t2l_ptr, &e.t2l_idx, &e.t2l_val, &e)))
         return rc;
     entries[n_entries] = e;
     *out = &entries[n_entries++];
@@ -419,6 +732,35 @@ int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, v
     return RPYB_OK;
 }
 
+int lie_project(int dtype, const Geometry& g, const LieMapsDev& maps, int64_t m, void* lie,
+                int64_t ld_lie, const void* x, int64_t ld_x, cudaStream_t s)
+{
+    if (m <= 0) return RPYB_OK;
+    const int64_t T = g.size(), L = maps.lie_dim;
+    ProjArgs a;
+    a.n_rows = L;
+    a.n_cols = T;
+    a.nnz = maps.t2l_nnz;
+    a.ntab = maps.t2l_ntab;
+    a.batch = m;
+    a.ld_y = ld_lie;
+    a.ld_x = ld_x;
+    a.pptr = maps.t2l_pptr;
+    a.ent = maps.t2l_ent;
+    a.tab = maps.t2l_tab;
+    if (maps.t2l_ent) {
+        if (dtype == RPYB_F64 && proj_smem_bytes<double>(a) <= (size_t)kProjSmemLimit)
+            return launch_lie_project<double>(a, lie, x, s);
+        if (dtype == RPYB_F32 && proj_smem_bytes<float>(a) <= (size_t)kProjSmemLimit)
+            return launch_lie_project<float>(a, lie, x, s);
+    }
+    // the sparse map accumulates: clear its outputs first
+    const size_t es = dtype == RPYB_F64 ? 8 : 4;
+    RPYB_CUDA(cudaMemset2DAsync(lie, (size_t)ld_lie * es, 0, (size_t)L * es, (size_t)m, s));
+    return rpyb_sparse_map(dtype, L, T, m, maps.t2l_ptr, maps.t2l_idx, maps.t2l_val, lie, x, ld_lie,
+                           ld_x, 1.0, s);
+}
+
 size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n)
 {
     n = std::max<int64_t>(n, 1);
@@ -430,8 +772,8 @@ size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n)
 }
 
 int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double* acc,
-                   double* out_logsig, int64_t ld_logsig, double* out_sig, int64_t ld_sig,
-                   void* scratch, size_t scratch_bytes, cudaStream_t s)
+                   bool acc_is_log, double* out_logsig, int64_t ld_logsig, double* out_sig,
+                   int64_t ld_sig, void* scratch, size_t scratch_bytes, cudaStream_t s)
 {
     if (m <= 0) return RPYB_OK;
     const int64_t T = g.size(), L = maps.lie_dim;
@@ -444,16 +786,16 @@ int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double*
     const size_t wsb = scratch_bytes - buf - lbuf;
     int rc;
     // log in float64 (its incoming out[0] must be zero), then tensor -> Lie
-    RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
-    if ((rc = rpyb_ft_log(RPYB_F64, g.width, g.depth, m, tmp, acc, T, T, -1, -1, ws, wsb, s)))
-        return rc;
+    const double* logt = acc;
+    if (!acc_is_log) {
+        RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
+        if ((rc = rpyb_ft_log(RPYB_F64, g.width, g.depth, m, tmp, acc, T, T, -1, -1, ws, wsb, s)))
+            return rc;
+        logt = tmp;
+    }
     double* lie = out_logsig ? out_logsig : lie_tmp;
     const int64_t ld_lie = out_logsig ? ld_logsig : L;
-    // the sparse map accumulates: clear its outputs first
-    RPYB_CUDA(cudaMemset2DAsync(lie, (size_t)(ld_lie * 8), 0, (size_t)(L * 8), (size_t)m, s));
-    if ((rc = rpyb_sparse_map(RPYB_F64, L, T, m, maps.t2l_ptr, maps.t2l_idx, maps.t2l_val, lie,
-                              tmp, ld_lie, T, 1.0, s)))
-        return rc;
+    if ((rc = lie_project(RPYB_F64, g, maps, m, lie, ld_lie, logt, T, s))) return rc;
     if (out_sig) {
         // algebra/src/context.cpp:156-159: exp(lie_to_tensor(log_signature))
         RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
@@ -524,11 +866,8 @@ RPYB_API int rpyb_tensor_to_lie(int dtype, int32_t width, int32_t depth, int64_t
     if (ld_out < L || ld_arg < g.size()) return fail(RPYB_E_INVALID, "row stride too small");
     const LieMapsDev* maps = nullptr;
     if ((rc = lie_maps_device(g, &maps))) return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const size_t es = dtype == RPYB_F64 ? 8 : 4;
-    RPYB_CUDA(cudaMemset2DAsync(out, (size_t)ld_out * es, 0, (size_t)L * es, (size_t)batch, s));
-    return rpyb_sparse_map(dtype, L, g.size(), batch, maps->t2l_ptr, maps->t2l_idx, maps->t2l_val,
-                           out, arg, ld_out, ld_arg, 1.0, s);
+    return lie_project(dtype, g, *maps, batch, out, ld_out, arg, ld_arg,
+                       static_cast<cudaStream_t>(stream));
 }
 
 RPYB_API int rpyb_lie_to_tensor(int dtype, int32_t width, int32_t depth, int64_t batch, void* out,

@@ -22,8 +22,20 @@ struct LieMapsDev {
     const int64_t* t2l_ptr = nullptr;   // lie_dim rows x tensor_size
     const int64_t* t2l_idx = nullptr;
     const double* t2l_val = nullptr;
+    // t2l packed for the shared-memory projection kernel (null when a column
+    // or the number of distinct values does not fit 16 bits): per entry
+    // column | (value id << 16), the distinct values in t2l_tab
+    const uint32_t* t2l_pptr = nullptr;   // lie_dim + 1
+    const uint32_t* t2l_ent = nullptr;
+    const double* t2l_tab = nullptr;
+    int64_t t2l_nnz = 0, t2l_ntab = 0;
 };
 int lie_maps_device(const Geometry& g, const LieMapsDev** out);
+
+// lie[b] <- t2l(x[b]) for m rows (assigning; dtype RPYB_F32 or RPYB_F64 for
+// both, float64 arithmetic)
+int lie_project(int dtype, const Geometry& g, const LieMapsDev& maps, int64_t m, void* lie,
+                int64_t ld_lie, const void* x, int64_t ld_x, cudaStream_t s);
 
 // rows idx[i] (or i) of `out` (stride ld) <- the unit tensor
 int unit_rows(int mode, void* out, int64_t ld, int64_t cols, const int64_t* idx, int64_t n,
@@ -38,23 +50,27 @@ int ordered_products(int acc_mode, int src_mode, const Geometry& g, int64_t n, v
                      const void* src, const std::vector<int64_t>& off,
                      const std::vector<int64_t>& src_rows, cudaStream_t s);
 
-// Same as ordered_products for a float64 accumulator, fused: one block per
-// row keeps acc[q] in shared memory across its whole list of factors.
-// Available for widths 2..6 and 8 with 2 * tensor_size * 8 <= 200 KB.
+// acc[q] <- src[r_0] * src[r_1] * ... (float64; the unit for an empty list),
+// or its float64 log when log_out is set (the log's Horner steps run in the
+// same block on the product still on the SM), fused: one block per row keeps
+// the running product on the SM across its whole list of factors (levels
+// below the top in shared memory, the top level in registers).  Available
+// for widths 2..6 and 8 when the top level fits the block's registers and
+// three copies of its lower levels 200 KB of shared memory.
 bool chain_products_available(const Geometry& g);
 int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                    const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
-                   cudaStream_t s);
+                   bool log_out, cudaStream_t s);
 
 // Bytes of scratch finish_queries needs for up to `n` rows.
 size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n);
 
-// For m group-like float64 rows `acc` ([m, T], overwritten): log-signature
-// t2l(log(acc)) into out_logsig and/or signature exp(l2t(logsig)) into
-// out_sig (either may be null).  Scratch from `scratch`.
+// For m group-like float64 rows `acc` ([m, T]; their logs when acc_is_log):
+// log-signature t2l(log(acc)) into out_logsig and/or signature
+// exp(l2t(logsig)) into out_sig (either may be null).  Scratch from `scratch`.
 int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double* acc,
-                   double* out_logsig, int64_t ld_logsig, double* out_sig, int64_t ld_sig,
-                   void* scratch, size_t scratch_bytes, cudaStream_t s);
+                   bool acc_is_log, double* out_logsig, int64_t ld_logsig, double* out_sig,
+                   int64_t ld_sig, void* scratch, size_t scratch_bytes, cudaStream_t s);
 
 // Stream::refine_interval (streams/src/stream.cpp:37-71) for a batch of
 // clopen queries against a support, then to_dyadic_intervals

@@ -274,3 +274,62 @@ def test_c_abi_build_rejects_unsorted_times_and_bad_rows():
     assert _lib.lib.rpyb_dyadic_build(_lib.F64, 3, 3, 2, 0.0, 1.0, 2, t.ctypes.data,
                                       rows.data_ptr(), 4, ctypes.byref(h), s) == _lib.E_INVALID
     assert not h.value
+
+
+@pytest.mark.parametrize("w,d", [(2, 12), (3, 8), (4, 6), (5, 4), (8, 4), (6, 5)])
+def test_c_abi_query_signatures_are_chen_products_of_events(w, d):
+    """Queries on the tree's grid (one or two top-level units per thread of the
+    fused chain-product kernel, widths 2..8): the signature of [a, b) equals
+    the signature of the events inside it, computed by the batched signature
+    kernel, and the log-signature equals t2l(log) of that signature; an empty
+    interval gives the unit and a zero log-signature."""
+    import torch
+    from roughpy_b200 import _lib
+    from roughpy_b200 import compute as rpc
+    from roughpy_b200 import signatures as S
+    rng = np.random.default_rng(w * 31 + d)
+    res, n = 6, 80
+    times = np.sort(rng.uniform(0, 1, n))
+    inc = torch.from_numpy(rng.normal(0, 0.05, (n, w))).cuda()
+    h = _build_raw(_lib.F64, w, d, res, 0.0, 1.0, times, inc)
+    try:
+        T = S.tensor_size(w, d)
+        lb, tb = rpc.LieBasis(w, d), rpc.TensorBasis(w, d)
+        L = lb.size()
+        grid = np.sort(rng.integers(0, 2 ** res + 1, (12, 2)), axis=1) / 2.0 ** res
+        grid[0] = [0.25, 0.25]
+        a, b = np.ascontiguousarray(grid[:, 0]), np.ascontiguousarray(grid[:, 1])
+        sig = torch.empty((12, T), dtype=torch.float64, device="cuda")
+        lie = torch.empty((12, L), dtype=torch.float64, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        _lib.check(_lib.lib.rpyb_dyadic_query(h, 12, a.ctypes.data, b.ctypes.data, res,
+                                              lie.data_ptr(), L, sig.data_ptr(), T, s))
+        got = sig.cpu().numpy()
+        unit = np.zeros(T)
+        unit[0] = 1.0
+        assert np.array_equal(got[0], unit)
+        assert not lie[0].any()
+        wants = []
+        for i in range(12):
+            sel = (times >= a[i]) & (times < b[i])
+            if not sel.any():
+                wants.append(torch.from_numpy(unit).cuda())
+                assert np.abs(got[i] - unit).max() <= 1e-13
+                continue
+            want = S.signature(inc[torch.from_numpy(sel).cuda()], None, d, "f64")[0]
+            wants.append(want)
+            # at depth 12 the top levels (~1e-14) come out of the log's Horner
+            # terms (~1e-5) by cancellation: the level-wise relative accuracy
+            # of the float64 log -> exp round trip is about 1e-10 there
+            tol = 1e-11 if d <= 8 else 2e-9
+            assert level_rel_err(got[i], want.cpu().numpy(), w, d) <= tol, i
+        # log-signatures: t2l(log(signature of the events))
+        W = torch.stack(wants)
+        lg = torch.zeros_like(W)
+        rpc._internals.dense_ft_log(lg, W, tb)
+        ref = torch.zeros((12, L), dtype=torch.float64, device="cuda")
+        rpc._internals.dense_tensor_to_lie(ref, lg, lb.get_t2l_matrix(), lb, tb)
+        scale = max(float(ref.abs().max()), 1e-300)
+        assert float((lie - ref).abs().max()) <= 1e-11 * scale
+    finally:
+        _lib.lib.rpyb_dyadic_free(h)

@@ -170,7 +170,7 @@ def test_lie_maps_on_gpu(golden):
         np.testing.assert_allclose(got, g[f"{t}_t2l_out"], rtol=0, atol=1e-12)
 
 
-@pytest.mark.parametrize("w,d", [(4, 4), (3, 5), (8, 3)])
+@pytest.mark.parametrize("w,d", [(4, 4), (3, 5), (8, 3), (6, 5)])
 def test_c_abi_tensor_lie_maps(w, d):
     """rpyb_tensor_to_lie / rpyb_lie_to_tensor (device-cached maps, assigning
     outputs) equal the roughpy.compute-style dense maps, and t2l(l2t(x)) = x
@@ -192,14 +192,53 @@ def test_c_abi_tensor_lie_maps(w, d):
     _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F64, w, d, 7, back.data_ptr(), L, emb.data_ptr(), T,
                                            s))
     assert float((back - x).abs().max()) <= 1e-13 * float(x.abs().max())
-    t = torch.from_numpy(rng.normal(size=(5, T))).cuda()
-    got = torch.empty((5, L), dtype=torch.float64, device="cuda")
-    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F64, w, d, 5, got.data_ptr(), L, t.data_ptr(), T, s))
-    ref = torch.zeros((5, L), dtype=torch.float64, device="cuda")
+    nb = 300   # more rows than blocks: each block projects several
+    t = torch.from_numpy(rng.normal(size=(nb, T))).cuda()
+    got = torch.empty((nb, L), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F64, w, d, nb, got.data_ptr(), L, t.data_ptr(), T,
+                                           s))
+    ref = torch.zeros((nb, L), dtype=torch.float64, device="cuda")
     rpc._internals.dense_tensor_to_lie(ref, t, lb.get_t2l_matrix(), lb, tb)
     assert float((got - ref).abs().max()) <= 1e-14 * float(ref.abs().max())
     t32 = t.float()
-    got32 = torch.empty((5, L), dtype=torch.float32, device="cuda")
-    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F32, w, d, 5, got32.data_ptr(), L, t32.data_ptr(), T,
-                                           s))
+    got32 = torch.empty((nb, L), dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib.rpyb_tensor_to_lie(_lib.F32, w, d, nb, got32.data_ptr(), L, t32.data_ptr(),
+                                           T, s))
     assert float((got32.double() - ref).abs().max()) <= 1e-6 * float(ref.abs().max())
+
+
+@pytest.mark.parametrize("batch", [7, 300])
+@pytest.mark.parametrize("n_rows,n_cols", [(97, 1500), (1960, 9331)])
+def test_c_abi_sparse_map_accumulates_with_strides(batch, n_rows, n_cols):
+    """rpyb_sparse_map, y += scale M x, in both dtypes, with row strides above
+    the sizes; entries whose column lies outside [0, n_cols) are skipped.
+    Checked against a float64 dense product."""
+    from roughpy_b200 import _lib
+    rng = np.random.default_rng(n_rows + batch)
+    nnz_row = rng.integers(0, 20, size=n_rows)
+    ptr = np.concatenate([[0], np.cumsum(nnz_row)]).astype(np.int64)
+    idx = rng.integers(0, n_cols, size=int(ptr[-1])).astype(np.int64)
+    val = rng.normal(size=int(ptr[-1]))
+    bad = rng.random(idx.shape[0]) < 0.05
+    idx[bad] = np.where(rng.random(int(bad.sum())) < 0.5, -1, n_cols)
+    M = np.zeros((n_rows, n_cols))
+    for r in range(n_rows):
+        for k in range(ptr[r], ptr[r + 1]):
+            if 0 <= idx[k] < n_cols:
+                M[r, idx[k]] += val[k]
+    x = rng.normal(size=(batch, n_cols + 5))
+    y0 = rng.normal(size=(batch, n_rows + 3))
+    d_ptr, d_idx, d_val = (torch.from_numpy(a).cuda() for a in (ptr, idx, val))
+    s = torch.cuda.current_stream().cuda_stream
+    for dt, code, tol in ((torch.float64, _lib.F64, 1e-12), (torch.float32, _lib.F32, 1e-5)):
+        xd = torch.from_numpy(x).to(dt).cuda()
+        yd = torch.from_numpy(y0).to(dt).cuda()
+        _lib.check(_lib.lib.rpyb_sparse_map(code, n_rows, n_cols, batch, d_ptr.data_ptr(),
+                                            d_idx.data_ptr(), d_val.data_ptr(), yd.data_ptr(),
+                                            xd.data_ptr(), n_rows + 3, n_cols + 5, 0.5, s))
+        torch.cuda.synchronize()
+        got = yd.double().cpu().numpy()
+        xr = xd.double().cpu().numpy()
+        ref = torch.from_numpy(y0).to(dt).double().numpy()
+        ref[:, :n_rows] += 0.5 * xr[:, :n_cols] @ M.T
+        assert np.abs(got - ref).max() <= tol * max(1.0, np.abs(ref).max())
