@@ -589,23 +589,25 @@ def profile_slice(n):
     print("profile slice done", n)
 
 
-def profile_queries(nq):
+def profile_queries(nq, log2_events=16):
     """The dyadic-query workload's tree (2^16 events, width 6, depth 5,
-    resolution 16, float32 nodes) and one query call of nq log-signatures: one
-    fused chain-product-and-log pass and one Hall projection per chunk of 8192
-    queries."""
+    resolution 16, float32 nodes; 2^log2_events events at resolution
+    log2_events for a smaller capture) and one query call of nq
+    log-signatures: one fused chain-product-and-log pass and one Hall
+    projection per chunk of 8192 queries."""
     import torch
     from roughpy_b200.streams import LieIncrementStream
-    n = 1 << 16
+    n = 1 << log2_events
     rng = np.random.default_rng(3)
     inc = rng.normal(0, np.sqrt(1.0 / n), size=(n, 6)).astype(np.float32)
     idx = np.arange(n) / n
     q = np.sort(np.floor(rng.uniform(0, 1, size=(nq, 2)) * n) / n, axis=1)
-    st = LieIncrementStream.from_increments(inc, indices=idx, width=6, depth=5, resolution=16)
+    st = LieIncrementStream.from_increments(inc, indices=idx, width=6, depth=5,
+                                            resolution=log2_events)
     st._build_tree()
     st.log_signature_batch(q[:, 0], q[:, 1])
     torch.cuda.synchronize()
-    print("profile queries done", nq)
+    print("profile queries done", nq, log2_events)
 
 
 def profile_fma(w, d, batch):
@@ -710,8 +712,9 @@ def main():
                     help="run one launch per mode on an N-stream slice and exit")
     ap.add_argument("--profile-fma", type=int, nargs=3, metavar=("WIDTH", "DEPTH", "BATCH"),
                     help="run one float64 and one float32 FMA launch and exit")
-    ap.add_argument("--profile-queries", type=int, default=0,
-                    help="build the dyadic-query tree, run N queries and exit")
+    ap.add_argument("--profile-queries", type=int, nargs="+", metavar=("N", "LOG2_EVENTS"),
+                    help="build the dyadic-query tree (2^16 events unless given), run N "
+                         "queries and exit")
     args = ap.parse_args()
     if args.profile_backward:
         profile_backward(args.profile_backward)
@@ -723,7 +726,7 @@ def main():
         profile_fma(*args.profile_fma)
         return
     if args.profile_queries:
-        profile_queries(args.profile_queries)
+        profile_queries(*args.profile_queries[:2])
         return
     if args.warmup < 3 and args.impl == "b200":
         log("note: warmup raised to 3")
