@@ -63,28 +63,65 @@ int upload(const std::vector<E>& h, const E** out)
     return RPYB_OK;
 }
 
-// the packed form of a CSR map (column | value id << 16 per entry); false
-// when a column or the number of distinct values does not fit 16 bits
+// The packed form of a CSR map for lie_project_kernel: rows sorted by entry
+// count (most first, stably) in groups of 32, each group padded to its
+// longest row with zero entries and stored lane-interleaved (entry j of lane
+// l at 32 j + l from the group's offset); an entry is column | value id << 16.
+// False when a column or the number of distinct values does not fit 16 bits.
 bool pack_csr(const std::vector<int64_t>& hp, const std::vector<int64_t>& hi,
-              const std::vector<double>& hv, int64_t nnz, int64_t n_cols,
-              std::vector<uint32_t>& pptr, std::vector<uint32_t>& ent, std::vector<double>& tab)
+              const std::vector<double>& hv, int64_t n_rows, int64_t n_cols,
+              std::vector<uint32_t>& goff, std::vector<uint32_t>& ent,
+              std::vector<uint32_t>& perm, std::vector<double>& tab)
 {
-    if (nnz >= ((int64_t)1 << 32) || n_cols > 0x10000) return false;
+    if (n_cols > 0x10000) return false;
     std::map<uint64_t, uint32_t> ids;   // keyed by the value's bits
-    pptr.assign(hp.begin(), hp.end());
-    ent.resize((size_t)nnz);
     tab.clear();
-    for (int64_t k = 0; k < nnz; ++k) {
-        if (hi[k] < 0 || hi[k] >= n_cols) return false;
+    auto id_of = [&](double v, uint32_t* out) {
         uint64_t bits;
-        std::memcpy(&bits, &hv[k], sizeof bits);
+        std::memcpy(&bits, &v, sizeof bits);
         auto it = ids.find(bits);
         if (it == ids.end()) {
             if (tab.size() > 0xffff) return false;
             it = ids.emplace(bits, (uint32_t)tab.size()).first;
-            tab.push_back(hv[k]);
+            tab.push_back(v);
         }
-        ent[k] = (uint32_t)hi[k] | (it->second << 16);
+        *out = it->second;
+        return true;
+    };
+    uint32_t zero_id = 0;
+    if (!id_of(0.0, &zero_id)) return false;
+    std::vector<int64_t> order(n_rows);
+    for (int64_t r = 0; r < n_rows; ++r) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+        return hp[x + 1] - hp[x] > hp[y + 1] - hp[y];
+    });
+    const int64_t groups = (n_rows + 31) / 32;
+    goff.assign(groups + 1, 0);
+    perm.assign(groups * 32, 0xffffffffu);
+    ent.clear();
+    for (int64_t g = 0; g < groups; ++g) {
+        int64_t len = 0;
+        for (int l = 0; l < 32 && g * 32 + l < n_rows; ++l) {
+            const int64_t r = order[g * 32 + l];
+            len = std::max<int64_t>(len, hp[r + 1] - hp[r]);
+            perm[g * 32 + l] = (uint32_t)r;
+        }
+        for (int64_t j = 0; j < len; ++j)
+            for (int l = 0; l < 32; ++l) {
+                uint32_t e = zero_id << 16;
+                if (g * 32 + l < n_rows) {
+                    const int64_t r = order[g * 32 + l];
+                    if (j < hp[r + 1] - hp[r]) {
+                        const int64_t k = hp[r] + j;
+                        uint32_t vid;
+                        if (hi[k] < 0 || hi[k] >= n_cols || !id_of(hv[k], &vid)) return false;
+                        e = (uint32_t)hi[k] | (vid << 16);
+                    }
+                }
+                ent.push_back(e);
+            }
+        if (ent.size() >= ((size_t)1 << 32)) return false;
+        goff[g + 1] = (uint32_t)ent.size();
     }
     return true;
 }
@@ -99,15 +136,17 @@ int upload_csr(const Geometry& g, int which, int64_t n_rows, const int64_t** ptr
     const int64_t got = rpyb_lie_map_csr(g.width, g.depth, which, hp.data(), hi.data(), hv.data());
     if (got < 0) return (int)got;
     if (packed_into) {
-        std::vector<uint32_t> pptr, ent;
+        std::vector<uint32_t> goff, ent, perm;
         std::vector<double> tab;
-        if (pack_csr(hp, hi, hv, nnz, g.size(), pptr, ent, tab)) {
+        if (pack_csr(hp, hi, hv, n_rows, g.size(), goff, ent, perm, tab)) {
             int rc;
-            if ((rc = upload(pptr, &packed_into->t2l_pptr)) ||
+            if ((rc = upload(goff, &packed_into->t2l_goff)) ||
                 (rc = upload(ent, &packed_into->t2l_ent)) ||
+                (rc = upload(perm, &packed_into->t2l_perm)) ||
                 (rc = upload(tab, &packed_into->t2l_tab)))
                 return rc;
-            packed_into->t2l_nnz = nnz;
+            packed_into->t2l_slots = (int64_t)ent.size();
+            packed_into->t2l_groups = (int64_t)goff.size() - 1;
             packed_into->t2l_ntab = (int64_t)tab.size();
         }
     }
@@ -166,26 +205,29 @@ int upload_async(void* dst, const void* src, size_t bytes, cudaStream_t s)
 // ------------------------------------------------------------------------
 // Tensor -> Lie projection with the packed map held in shared memory.  One
 // persistent block per SM loads the map (column and value id per entry, the
-// distinct values, the row pointers) once; for each of its rows of x it
-// copies the row into shared memory with coalesced loads and computes every
-// Lie coordinate from shared memory.  The compact entries are what makes
-// this pay: as (int64, float64) pairs the map is larger than a row of x and
-// its gathers go to L2 for every row.
+// distinct values, the group offsets) once; for each of its rows of x it
+// copies the row into shared memory with coalesced loads, and every warp
+// computes groups of 32 Lie coordinates from shared memory, one per lane.
+// The compact entries are what makes this pay: as (int64, float64) pairs the
+// map is larger than a row of x and its gathers go to L2 for every row.  The
+// lane-interleaved groups make a warp's entry reads consecutive words and
+// give its lanes equal trip counts.
 constexpr int kProjThreads = 1024;
 constexpr int64_t kProjSmemLimit = 220 * 1024;
 
 struct ProjArgs {
-    int64_t n_rows = 0, n_cols = 0, nnz = 0, ntab = 0, batch = 0;
+    int64_t n_cols = 0, slots = 0, groups = 0, ntab = 0, batch = 0;
     int64_t ld_y = 0, ld_x = 0;
-    const uint32_t* pptr = nullptr;
+    const uint32_t* goff = nullptr;
     const uint32_t* ent = nullptr;
+    const uint32_t* perm = nullptr;
     const double* tab = nullptr;
 };
 
 template <typename T>
 size_t proj_smem_bytes(const ProjArgs& a)
 {
-    return (size_t)(a.ntab * 8 + a.n_cols * (int64_t)sizeof(T) + (a.n_rows + 1) * 4 + a.nnz * 4);
+    return (size_t)(a.ntab * 8 + a.n_cols * (int64_t)sizeof(T) + (a.groups + 1) * 4 + a.slots * 4);
 }
 
 template <typename T>
@@ -195,12 +237,13 @@ lie_project_kernel(const ProjArgs a, T* __restrict__ y, const T* __restrict__ x)
     extern __shared__ __align__(16) unsigned char proj_smem[];
     double* tab = reinterpret_cast<double*>(proj_smem);
     T* xs = reinterpret_cast<T*>(tab + a.ntab);
-    uint32_t* pptr = reinterpret_cast<uint32_t*>(xs + a.n_cols);
-    uint32_t* ent = pptr + a.n_rows + 1;
+    uint32_t* goff = reinterpret_cast<uint32_t*>(xs + a.n_cols);
+    uint32_t* ent = goff + a.groups + 1;
     const int tid = (int)threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = (int)blockDim.x >> 5;
     for (int64_t i = tid; i < a.ntab; i += blockDim.x) tab[i] = a.tab[i];
-    for (int64_t i = tid; i <= a.n_rows; i += blockDim.x) pptr[i] = a.pptr[i];
-    for (int64_t i = tid; i < a.nnz; i += blockDim.x) ent[i] = a.ent[i];
+    for (int64_t i = tid; i <= a.groups; i += blockDim.x) goff[i] = a.goff[i];
+    for (int64_t i = tid; i < a.slots; i += blockDim.x) ent[i] = a.ent[i];
     constexpr int kU = 8;
     for (int64_t b = blockIdx.x; b < a.batch; b += gridDim.x) {
         __syncthreads();   // the map is loaded; the previous row's gathers are done
@@ -228,14 +271,16 @@ lie_project_kernel(const ProjArgs a, T* __restrict__ y, const T* __restrict__ x)
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + l));
         }
         T* yr = y + b * a.ld_y;
-        for (int64_t r = tid; r < a.n_rows; r += blockDim.x) {
+        for (int64_t g = warp; g < a.groups; g += nwarps) {
             double acc = 0.0;
-            const uint32_t e = pptr[r + 1];
-            for (uint32_t k = pptr[r]; k < e; ++k) {
+            const uint32_t e1 = goff[g + 1];
+#pragma unroll 4
+            for (uint32_t k = goff[g] + lane; k < e1; k += 32) {
                 const uint32_t w = ent[k];
                 acc = fma(tab[w >> 16], (double)xs[w & 0xffffu], acc);
             }
-            yr[r] = (T)acc;
+            const uint32_t row = __ldg(a.perm + g * 32 + lane);
+            if (row != 0xffffffffu) yr[row] = (T)acc;
         }
     }
 }
@@ -289,14 +334,18 @@ constexpr int kChainThreads = 512;
 
 // out[D][V] (+)= sum over s = 1..k-1 of lhs level k-s (x) rhs level s at the
 // unit (rp, c0) of level k: the left factor's D words of first letters u at
-// middle part rp's prefix, the right factor's V words after it
-template <int D, int V, typename TR, bool GLOBAL_RHS>
+// middle part rp's prefix, the right factor's V words after it.  KC > 0 fixes
+// k = KC at compile time; the loop is then unrolled, which lets the loads of
+// all split points be issued together.
+template <int D, int V, typename TR, bool GLOBAL_RHS, int KC = 0>
 __device__ __forceinline__ void unit_splits(double (&acc)[D][V], const double* lhs, const TR* rhs,
                                             const ChainArgs& a, int k, uint32_t rp, int c0)
 {
     uint32_t qq = rp;
     uint32_t m = 0;
-    for (int s = 1; s <= k - 1; ++s) {
+    if constexpr (KC > 0) k = KC;
+#pragma unroll
+    for (int s = 1; s <= (KC > 0 ? KC : k) - 1; ++s) {
         const int p = k - s;
         double lv[D];
         double rv[V];
@@ -335,7 +384,8 @@ __device__ __forceinline__ void lower_unit(const ChainArgs& a, int64_t li, int& 
     obase = a.db[k] + (int64_t)rp * D + c0;
 }
 
-template <typename TS, int D, int V, int TU>
+// NT > 0: the depth is NT (the top level's split loop is unrolled)
+template <typename TS, int D, int V, int TU, int NT>
 __global__ void __launch_bounds__(kChainThreads, 1)
 chain_products_kernel(const ChainArgs a)
 {
@@ -406,7 +456,7 @@ chain_products_kernel(const ChainArgs a)
                 for (int u = 0; u < D; ++u)
 #pragma unroll
                     for (int j = 0; j < V; ++j) top[t][u][j] *= node0;
-                unit_splits<D, V, TS, true>(top[t], cur, node, a, N, trp[t], tc0[t]);
+                unit_splits<D, V, TS, true, NT>(top[t], cur, node, a, N, trp[t], tc0[t]);
 #pragma unroll
                 for (int u = 0; u < D; ++u)
 #pragma unroll
@@ -461,7 +511,8 @@ chain_products_kernel(const ChainArgs a)
                         for (int u = 0; u < D; ++u)
 #pragma unroll
                             for (int j = 0; j < V; ++j) top[t][u][j] *= c;
-                        unit_splits<D, V, double, false>(top[t], rc, cur, a, N, trp[t], tc0[t]);
+                        unit_splits<D, V, double, false, NT>(top[t], rc, cur, a, N, trp[t],
+                                                             tc0[t]);
                     }
                 }
                 for (int64_t f = f_low; f < a.utop + a.ulow; f += B) {
@@ -530,25 +581,34 @@ int chain_tu(const Geometry& g)
 
 using ChainFn = void (*)(ChainArgs);
 
-template <typename TS>
-ChainFn chain_fn(int width, int tu)
+template <typename TS, int NT>
+ChainFn chain_fn_nt(int width, int tu)
 {
     if (tu == 2) {
         switch (width) {
-            case 2: return &chain_products_kernel<TS, 2, 2, 2>;
-            case 3: return &chain_products_kernel<TS, 3, 3, 2>;
+            case 2: return &chain_products_kernel<TS, 2, 2, 2, NT>;
+            case 3: return &chain_products_kernel<TS, 3, 3, 2, NT>;
             default: return nullptr;
         }
     }
     switch (width) {
-        case 2: return &chain_products_kernel<TS, 2, 2, 1>;
-        case 3: return &chain_products_kernel<TS, 3, 3, 1>;
-        case 4: return &chain_products_kernel<TS, 4, 4, 1>;
-        case 5: return &chain_products_kernel<TS, 5, 1, 1>;
-        case 6: return &chain_products_kernel<TS, 6, 3, 1>;
-        case 8: return &chain_products_kernel<TS, 8, 2, 1>;
+        case 2: return &chain_products_kernel<TS, 2, 2, 1, NT>;
+        case 3: return &chain_products_kernel<TS, 3, 3, 1, NT>;
+        case 4: return &chain_products_kernel<TS, 4, 4, 1, NT>;
+        case 5: return &chain_products_kernel<TS, 5, 1, 1, NT>;
+        case 6: return &chain_products_kernel<TS, 6, 3, 1, NT>;
+        case 8: return &chain_products_kernel<TS, 8, 2, 1, NT>;
         default: return nullptr;
     }
+}
+
+// depths 5 and 6 get a kernel with the top level's split loop unrolled
+template <typename TS>
+ChainFn chain_fn(int width, int depth, int tu)
+{
+    if (depth == 5) return chain_fn_nt<TS, 5>(width, tu);
+    if (depth == 6) return chain_fn_nt<TS, 6>(width, tu);
+    return chain_fn_nt<TS, 0>(width, tu);
 }
 
 constexpr int64_t kChainSmemLimit = 200 * 1024;
@@ -605,7 +665,8 @@ int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, cons
     a.log_out = log_out ? 1 : 0;
     const size_t smem = (size_t)((log_out ? 3 : 2) * g.db[g.depth] * 8);
     const unsigned grid = (unsigned)std::min<int64_t>(n, 1 << 20);
-    ChainFn fn = src_mode == RPYB_F64 ? chain_fn<double>(g.width, tu) : chain_fn<float>(g.width, tu);
+    ChainFn fn = src_mode == RPYB_F64 ? chain_fn<double>(g.width, g.depth, tu)
+                                      : chain_fn<float>(g.width, g.depth, tu);
     if (smem > 48 * 1024)
         RPYB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     fn<<<grid, kChainThreads, smem, s>>>(a);
@@ -738,15 +799,16 @@ int lie_project(int dtype, const Geometry& g, const LieMapsDev& maps, int64_t m,
     if (m <= 0) return RPYB_OK;
     const int64_t T = g.size(), L = maps.lie_dim;
     ProjArgs a;
-    a.n_rows = L;
     a.n_cols = T;
-    a.nnz = maps.t2l_nnz;
+    a.slots = maps.t2l_slots;
+    a.groups = maps.t2l_groups;
     a.ntab = maps.t2l_ntab;
     a.batch = m;
     a.ld_y = ld_lie;
     a.ld_x = ld_x;
-    a.pptr = maps.t2l_pptr;
+    a.goff = maps.t2l_goff;
     a.ent = maps.t2l_ent;
+    a.perm = maps.t2l_perm;
     a.tab = maps.t2l_tab;
     if (maps.t2l_ent) {
         if (dtype == RPYB_F64 && proj_smem_bytes<double>(a) <= (size_t)kProjSmemLimit)

@@ -23,12 +23,17 @@ struct LieMapsDev {
     const int64_t* t2l_idx = nullptr;
     const double* t2l_val = nullptr;
     // t2l packed for the shared-memory projection kernel (null when a column
-    // or the number of distinct values does not fit 16 bits): per entry
-    // column | (value id << 16), the distinct values in t2l_tab
-    const uint32_t* t2l_pptr = nullptr;   // lie_dim + 1
+    // or the number of distinct values does not fit 16 bits).  Rows sorted by
+    // entry count, in groups of 32 (one per warp lane), each group padded to
+    // its longest row; entry j of lane l of group g is t2l_ent[t2l_goff[g] +
+    // 32 j + l] = column | (value id << 16), the distinct values (and a zero
+    // for the padding) in t2l_tab; t2l_perm[32 g + l] is the lane's row, or
+    // 0xffffffff past the last row.
+    const uint32_t* t2l_goff = nullptr;   // groups + 1
     const uint32_t* t2l_ent = nullptr;
+    const uint32_t* t2l_perm = nullptr;   // 32 * groups
     const double* t2l_tab = nullptr;
-    int64_t t2l_nnz = 0, t2l_ntab = 0;
+    int64_t t2l_slots = 0, t2l_groups = 0, t2l_ntab = 0;
 };
 int lie_maps_device(const Geometry& g, const LieMapsDev** out);
 
