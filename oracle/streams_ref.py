@@ -274,3 +274,100 @@ class PiecewiseRef:
 
     def signature(self, inf=None, sup=None, resolution=None):
         return self.a.to_signature(self.log_signature(inf, sup, resolution))
+
+
+class TickRef:
+    """TickStream restated (streams/src/tick_stream.cpp:41-201 with
+    streams/include/roughpy/streams/tick_stream.h:66-83), queried through the
+    Stream rules (streams/src/stream.cpp:37-171, stream_base.cpp:81-96).
+    Clopen intervals.
+
+    Events (time, Lie coordinates) are keyed by their dyadic interval at the
+    stream resolution; events sharing one are combined by CBH in input order.
+    The cache holds, for the sub-intervals visited by the recursion from the
+    smallest dyadic intervals containing all negative and all positive events,
+    the CBH of the two halves; a dyadic query piece takes the cached value of
+    the smallest dyadic interval containing the events inside it."""
+
+    def __init__(self, arith, events, resolution=0, support=(0.0, 1.0)):
+        self.a = arith
+        self.resolution = int(resolution)
+        self.support = (float(support[0]), float(support[1]))
+        R = self.resolution
+        self.data = {}
+        index = set()
+        for t, lie in events:
+            k = math.floor(math.ldexp(float(t), R))
+            lie = np.asarray(lie, dtype=np.float64)
+            full = np.zeros(arith.L)
+            full[:lie.shape[0]] = lie
+            if (k, R) in self.data:
+                self.data[(k, R)] = arith.cbh([self.data[(k, R)], full])
+            else:
+                self.data[(k, R)] = full
+            index.add(math.ldexp(k, -R))
+        self.granular = sorted(index)
+        # tick_stream.cpp:60-98: the negative events are those at or before
+        # 0, the positive ones those from the first leaf start >= 0 (a clopen
+        # leaf at 0 ends above 0), so the leaf at 0 belongs to both
+        neg = self._smallest_of_range(0, bisect.bisect_right(self.granular, 0.0))
+        pos = self._smallest_of_range(bisect.bisect_left(self.granular, 0.0),
+                                      len(self.granular))
+        for root in (neg, pos):
+            if root is not None:
+                self._recursive(root)
+
+    def _leaf(self, t):
+        R = self.resolution
+        return (math.floor(math.ldexp(t, R)), R)
+
+    def _smallest_of_range(self, lo, hi):
+        # tick_stream.cpp:41-98: expand the first event's leaf until it
+        # contains the last event's leaf
+        if hi <= lo:
+            return None
+        k, p = self._leaf(self.granular[lo])
+        ek, ep = self._leaf(self.granular[hi - 1])
+        steps = 0
+        while not _contains(k, p, ek, ep):
+            k, p = _from_dyadic(k, p, p - 1)
+            steps += 1
+            if steps > 4 * 64:
+                # a range from before 0 to the leaf at 0: k stays -1 and the
+                # reference's loop does not end
+                raise ValueError("no dyadic interval contains events on both sides of 0")
+        return (k, p)
+
+    def _smallest(self, k, p):
+        inf, sup = math.ldexp(k, -p), math.ldexp(k + 1, -p)
+        lo = bisect.bisect_left(self.granular, inf)
+        hi = bisect.bisect_left(self.granular, sup)
+        return self._smallest_of_range(lo, hi)
+
+    def _recursive(self, di):
+        # tick_stream.cpp:100-123
+        s = self._smallest(*di)
+        if s is None:
+            return np.zeros(self.a.L)
+        it = self.data.get(s)
+        if it is not None and np.any(it):
+            return it
+        if s[1] == self.resolution:
+            self.data.setdefault(s, np.zeros(self.a.L))
+            return self.data[s]
+        left = self._recursive((2 * s[0], s[1] + 1))
+        right = self._recursive((2 * s[0] + 1, s[1] + 1))
+        self.data[s] = self.a.cbh([left, right])
+        return self.data[s]
+
+    def _dyadic_logsig(self, k, p):
+        # tick_stream.cpp:188-201 (log_signature_impl)
+        s = self._smallest(k, p)
+        if s is None:
+            return np.zeros(self.a.L)
+        return self.data[s]
+
+    log_signature = StreamRef.log_signature
+
+    def signature(self, inf=None, sup=None, resolution=None):
+        return self.a.to_signature(self.log_signature(inf, sup, resolution))

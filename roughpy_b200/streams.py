@@ -46,7 +46,7 @@ from . import compute as rpc
 from . import signatures as S
 
 __all__ = ["RealInterval", "DyadicInterval", "to_dyadic_intervals", "LieIncrementStream",
-           "PiecewiseAbelianStream", "param_to_resolution", "sig_derivative",
+           "TickStream", "PiecewiseAbelianStream", "param_to_resolution", "sig_derivative",
            "sig_derivative_batch"]
 
 
@@ -354,6 +354,69 @@ class LieIncrementStream(_StreamQueries):
                 lie.data_ptr() if logsig else None, L, sg.data_ptr() if sig else None, T,
                 stream))
         return lie, sg
+
+
+class TickStream(LieIncrementStream):
+    """Tick stream (streams/src/tick_stream.cpp:41-201,
+    streams/include/roughpy/streams/tick_stream.h:66-83): events (time, Lie
+    coordinates) keyed by their dyadic interval at the stream resolution.
+    Events sharing an interval are combined in input order and are not
+    de-duplicated by time; a dyadic query piece takes the log-signature of
+    the events inside it (the reference looks up the cached CBH of the
+    smallest dyadic interval holding them), and the pieces are combined as
+    for every stream (streams/src/stream.cpp:37-171).
+
+    On the device this is the dyadic signature tree of the events sorted
+    stably by interval, each placed at its interval's start: a leaf is the
+    product of exp over its events in input order, every node the product of
+    the events inside it, so the queries are those of LieIncrementStream.
+    The reference's construction does not terminate when there are events
+    both before 0 and in the interval starting at 0 (its search for the
+    smallest interval holding the negative events cannot pass 0); that case
+    has a well-defined answer here."""
+
+    @classmethod
+    def from_lie_events(cls, times, data, width, depth, resolution=0, support=None, dtype=None,
+                        mode=None, device="cuda"):
+        """The stream of events (times[i], data[i]), in input order.
+
+        ``data``: rows of Lie coordinates (the first ``width`` are the letters;
+        further entries are higher Hall-basis coordinates).  ``resolution``
+        and ``support`` default as in the reference's tick-stream
+        constructor: 0 and [0, 1) (roughpy/src/streams/tick_stream.cpp:131-141).
+        """
+        rows = np.asarray(data)
+        if rows.ndim == 1:
+            rows = rows.reshape(1, -1)
+        if rows.ndim != 2:
+            raise ValueError("tick data must be a two-dimensional array")
+        t = np.asarray(times, dtype=np.float64).reshape(-1)
+        if t.shape[0] != rows.shape[0]:
+            raise ValueError("mismatch between number of rows in data and number of times")
+        if t.shape[0] == 0:
+            raise ValueError("tick data cannot be empty")
+        if dtype is None:
+            dtype = np.float32 if rows.dtype == np.float32 else np.float64
+        lie_dim = rpc.LieBasis(width, depth).size()
+        ncol = min(rows.shape[1], lie_dim)
+        lies = np.zeros((rows.shape[0], max(ncol, width)), dtype=np.float64)
+        lies[:, :ncol] = rows[:, :ncol]
+        res = int(resolution)
+        # DyadicInterval(t, resolution): [floor(t 2^res), +1) / 2^res
+        k = np.floor(np.ldexp(t, res))
+        order = np.argsort(k, kind="stable")
+        starts = np.ldexp(k[order], -res)
+        if support is None:
+            support = RealInterval(0.0, 1.0)
+        elif not isinstance(support, RealInterval):
+            support = RealInterval(*support)
+        return cls(starts, lies[order], width, depth, res, support, dtype, mode, device)
+
+    @classmethod
+    def from_data(cls, *args, **kwargs):
+        raise NotImplementedError(
+            "tick data parsing (labels, channel types, schemas) is not provided; build the "
+            "stream from (time, Lie coordinates) events with TickStream.from_lie_events")
 
 
 class PiecewiseAbelianStream(_StreamQueries):

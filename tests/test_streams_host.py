@@ -170,3 +170,49 @@ def test_restated_piecewise_full_data_is_cbh_of_the_pieces(golden, count):
         lies.append(v)
     st = R.PiecewiseRef(a, [(float(i), float(i + 1), v) for i, v in enumerate(lies)])
     np.testing.assert_array_almost_equal(st.log_signature(resolution=5), a.cbh(lies), decimal=12)
+
+
+def test_tick_restatement_known_answer(golden):
+    """Two increments at one time step, combined by CBH in input order
+    (tests/streams/test_tick_stream.py:107-115 expects Lie([1, 1, 0.5]) for
+    "first" then "second"); the reverse order flips the bracket."""
+    a = arith(golden, 2, 2)
+    e1, e2 = [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]
+    t = R.TickRef(a, [(1.0, e1), (1.0, e2)], resolution=0, support=(0.0, 2.0))
+    np.testing.assert_allclose(t.log_signature(0.0, 2.0, 2), [1.0, 1.0, 0.5], atol=1e-15)
+    t = R.TickRef(a, [(1.0, e2), (1.0, e1)], resolution=0, support=(0.0, 2.0))
+    np.testing.assert_allclose(t.log_signature(0.0, 2.0, 2), [1.0, 1.0, -0.5], atol=1e-15)
+
+
+@pytest.mark.parametrize("w,d", [(2, 3), (3, 3)])
+def test_tick_restatement_matches_the_cached_stream_on_distinct_times(golden, w, d):
+    """With one event per leaf, in time order, the tick stream's compressed
+    recursion and the caching layer's cached leaves give the same
+    log-signatures on every query (both are the CBH of the events inside)."""
+    a = arith(golden, w, d)
+    rng = np.random.default_rng(w + 10 * d)
+    res = 4
+    # no event in the leaf at 0 next to negative ones (the reference's
+    # construction does not end for that case)
+    cand = np.concatenate([np.arange(-20, 0), np.arange(1, 40)])
+    leaves = np.sort(rng.choice(cand, size=15, replace=False))
+    times = leaves / 2.0 ** res + rng.uniform(0, 1, 15) / 2.0 ** (res + 1)
+    rows = rng.normal(0, 0.3, (15, a.L))
+    support = (float(times.min()), float(times.max()) + 2.0 ** -res)
+    tick = R.TickRef(a, [(t, r) for t, r in zip(times, rows)], resolution=res, support=support)
+    ref = R.StreamRef(a, rows, indices=times, resolution=res)
+    ref.support = support
+    for _ in range(30):
+        lo, hi = np.sort(rng.uniform(support[0] - 0.2, support[1] + 0.2, 2))
+        for q_res in (None, res - 2, res + 2):
+            np.testing.assert_allclose(tick.log_signature(lo, hi, q_res),
+                                       ref.log_signature(lo, hi, q_res), atol=1e-12)
+
+
+def test_tick_restatement_rejects_events_on_both_sides_of_zero_leaf(golden):
+    """The reference's search for the smallest dyadic interval holding events
+    before 0 and in the leaf at 0 never ends (k stays -1); the restatement
+    raises instead."""
+    a = arith(golden, 2, 2)
+    with pytest.raises(ValueError):
+        R.TickRef(a, [(-0.5, [1.0, 0.0, 0.0]), (0.25, [0.0, 1.0, 0.0])], resolution=0)
