@@ -216,3 +216,27 @@ def test_tick_restatement_rejects_events_on_both_sides_of_zero_leaf(golden):
     a = arith(golden, 2, 2)
     with pytest.raises(ValueError):
         R.TickRef(a, [(-0.5, [1.0, 0.0, 0.0]), (0.25, [0.0, 1.0, 0.0])], resolution=0)
+
+
+def test_tick_stream_event_layout_for_the_tree():
+    """TickStream.from_lie_events (host side, nothing on the device until the
+    first query): events are ordered stably by their dyadic interval at the
+    stream resolution, keep their input order inside an interval (no
+    de-duplication by time) and sit at the interval's start; the defaults
+    are resolution 0 and support [0, 1); bad inputs are rejected."""
+    from roughpy_b200.streams import TickStream
+    times = [0.30, 0.10, 0.27, 0.26, -0.05, 0.10]
+    rows = np.arange(12.0).reshape(6, 2)
+    st = TickStream.from_lie_events(times, rows, 2, 2, resolution=2, support=(-1.0, 1.0))
+    # intervals at resolution 2: 1, 0, 1, 1, -1, 0
+    np.testing.assert_array_equal(st.times, [-0.25, 0.0, 0.0, 0.25, 0.25, 0.25])
+    np.testing.assert_array_equal(st.lies[:, :2], rows[[4, 1, 5, 0, 2, 3]])
+    assert (st.support.inf, st.support.sup) == (-1.0, 1.0)
+    st = TickStream.from_lie_events([0.5], [[1.0, 2.0]], 2, 2)
+    assert st.resolution == 0 and (st.support.inf, st.support.sup) == (0.0, 1.0)
+    with pytest.raises(ValueError):
+        TickStream.from_lie_events([0.1, 0.2], [[1.0, 2.0]], 2, 2)
+    with pytest.raises(ValueError):
+        TickStream.from_lie_events([], np.zeros((0, 2)), 2, 2)
+    with pytest.raises(NotImplementedError):
+        TickStream.from_data({1.0: [("a", "increment", 1.0)]}, width=2, depth=2)
