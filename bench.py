@@ -403,6 +403,11 @@ def plain_f64_signatures(dev):
     got = out.cpu().numpy()
     want = oracle.signatures(w, d, inc[:16 * L], off[:17])
     err = float(np.max(np.abs(got[:16] - want)) / np.max(np.abs(want)))
+    # the same launch replayed from a CUDA graph (no per-call launch overhead)
+    graph, gout = plan.capture(x)
+    ms_graph = _events_time(torch, graph.replay, 50)
+    graph_same = bool(torch.equal(gout, out))
+    del graph
     ref = {}
     rpc = oracle.ref_compute()
     if rpc is not None:
@@ -413,6 +418,8 @@ def plain_f64_signatures(dev):
                "sample": "32 of the 256 streams, chained roughpy.compute ft_fmexp"}
     return {"workload": "256 streams x 128 increments, width 4, depth 5, float64",
             "value": round(n / (ms / 1e3), 1), "unit": "streams/s", "ms": round(ms, 4),
+            "cuda_graph": {"value": round(n / (ms_graph / 1e3), 1), "ms": round(ms_graph, 4),
+                           "same_output": graph_same},
             "max_rel_err_vs_oracle": err, "cpu_reference_1_core": ref}
 
 

@@ -32,6 +32,8 @@
 // when folding, which leaves the registers to the delta accumulators.
 #include <algorithm>
 #include <mutex>
+#include <tuple>
+#include <map>
 #include <vector>
 
 #include "common.cuh"
@@ -663,29 +665,43 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
         // Warps are independent, so the block size only matters for occupancy:
         // take the block size that fits the most warps per SM (registers and
         // shared memory are both per-warp here), preferring larger blocks.
-        static std::mutex mu;
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(smem_warp * kSigWarps)));
-        }
+        // The attribute and the choice are made once per device, kernel and
+        // per-warp shared memory, so repeated launches (and a launch captured
+        // into a CUDA graph) only reset the queue and launch.
         int wpb = signature_warps_per_block();
         int per_sm = 0;
-        if (wpb == 0) {
-            int best_warps = -1;
-            for (int w = kSigWarps; w >= 1; --w) {
-                int bps = 0;
-                RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, v.fn, w * 32,
-                                                                        smem_warp * w));
-                if (bps * w > best_warps) {
-                    best_warps = bps * w;
-                    wpb = w;
-                    per_sm = bps;
+        {
+            static std::mutex mu;
+            static std::map<std::tuple<int, const void*, size_t>, std::pair<int, int>> chosen;
+            int dev = 0;
+            RPYB_CUDA(cudaGetDevice(&dev));
+            std::lock_guard<std::mutex> lk(mu);
+            const auto key = std::make_tuple(dev, (const void*)v.fn, smem_warp);
+            auto it = chosen.find(key);
+            if (it == chosen.end()) {
+                RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(smem_warp * kSigWarps)));
+                int best_wpb = wpb, best_per_sm = 0;
+                if (wpb == 0) {
+                    int best_warps = -1;
+                    for (int w = kSigWarps; w >= 1; --w) {
+                        int bps = 0;
+                        RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, v.fn, w * 32,
+                                                                                smem_warp * w));
+                        if (bps * w > best_warps) {
+                            best_warps = bps * w;
+                            best_wpb = w;
+                            best_per_sm = bps;
+                        }
+                    }
+                } else {
+                    RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &best_per_sm, v.fn, wpb * 32, smem_warp * wpb));
                 }
+                it = chosen.emplace(key, std::make_pair(best_wpb, best_per_sm)).first;
             }
-        } else {
-            RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, wpb * 32,
-                                                                    smem_warp * wpb));
+            wpb = it->second.first;
+            per_sm = it->second.second;
         }
         if (per_sm < 1) per_sm = 1;
         const size_t smem = smem_warp * wpb;

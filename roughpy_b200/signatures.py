@@ -97,6 +97,29 @@ class SignaturePlan:
             self.order.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(), s))
         return out
 
+    def capture(self, increments: torch.Tensor, out: torch.Tensor | None = None):
+        """Capture one launch into a CUDA graph: returns ``(graph, out)``.
+
+        ``increments`` and ``out`` become the graph's static buffers: refill
+        ``increments`` in place (same layout) and call ``graph.replay()`` to
+        recompute ``out``.  A launch is a work-queue reset and one persistent
+        kernel on the plan's own workspace, so the graph holds no allocation;
+        what replay saves is the per-call launch overhead, which dominates for
+        small batches.  The first launch runs outside the capture, on a side
+        stream, so that one-time set-up (module loading, kernel attributes)
+        stays out of the graph."""
+        if out is None:
+            out = torch.empty((self.n_streams, self.size), dtype=self.dtype, device=self.device)
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self.run(increments, out, stream=side)
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self.run(increments, out)
+        return graph, out
+
     def run_host_pipelined(self, inc_host: torch.Tensor, out_host: torch.Tensor,
                            n_chunks: int = 8) -> torch.Tensor:
         """End-to-end call on host buffers through ``rpyb_signature_host``:

@@ -93,3 +93,24 @@ def test_host_pipelined_entry_matches_device_path(mode, chunks):
     plan.run_host_pipelined(inc_h, out_h, n_chunks=chunks)
     torch.cuda.synchronize()
     assert torch.equal(out_h, want)
+
+
+@pytest.mark.parametrize("mode", ["f64", "f32c"])
+def test_plan_cuda_graph_replays_with_refilled_inputs(mode):
+    """SignaturePlan.capture: the captured launch, replayed after refilling
+    the static increments in place, gives exactly the direct launch's result
+    on the new increments; two replays in a row."""
+    rng = np.random.default_rng(8)
+    w, d = 4, 5
+    lens = rng.integers(0, 300, size=40)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    plan = S.SignaturePlan(off, w, d, mode)
+    x = torch.from_numpy(rng.normal(0, 0.1, size=(int(off[-1]), w))).to("cuda", plan.dtype)
+    graph, gout = plan.capture(x)
+    for trial in range(2):
+        new = torch.from_numpy(rng.normal(0, 0.1, size=(int(off[-1]), w))).to("cuda", plan.dtype)
+        x.copy_(new)
+        graph.replay()
+        want = plan.run(new)
+        torch.cuda.synchronize()
+        assert torch.equal(gout, want), trial
