@@ -35,6 +35,7 @@ rules (event de-duplication, the resolution heuristic, the default support).
 """
 from __future__ import annotations
 
+import copy
 import ctypes
 import math
 
@@ -45,9 +46,9 @@ from . import _lib
 from . import compute as rpc
 from . import signatures as S
 
-__all__ = ["RealInterval", "DyadicInterval", "to_dyadic_intervals", "LieIncrementStream",
-           "TickStream", "PiecewiseAbelianStream", "param_to_resolution", "sig_derivative",
-           "sig_derivative_batch"]
+__all__ = ["RealInterval", "DyadicInterval", "Partition", "to_dyadic_intervals",
+           "LieIncrementStream", "TickStream", "PiecewiseAbelianStream", "param_to_resolution",
+           "sig_derivative", "sig_derivative_batch"]
 
 
 class RealInterval:
@@ -62,6 +63,46 @@ class RealInterval:
 
     def __repr__(self):
         return f"[{self.inf}, {self.sup})"
+
+
+class Partition:
+    """A clopen interval cut at intermediate points (intervals/src/partition.cpp:
+    the points strictly inside the interval are kept, sorted, duplicates
+    included); ``partition[i]`` is the i-th sub-interval."""
+
+    def __init__(self, interval, intermediates=()):
+        inf, sup = ((interval.inf, interval.sup) if isinstance(interval, (RealInterval,))
+                    else (float(interval[0]), float(interval[1])))
+        self.inf, self.sup = float(inf), float(sup)
+        self._points = sorted(float(m) for m in intermediates
+                              if self.inf <= float(m) < self.sup and float(m) != self.inf)
+
+    def __len__(self):
+        return len(self._points) + 1
+
+    def __getitem__(self, i):
+        n = len(self._points)
+        if i < 0:
+            i += n + 1
+        if not 0 <= i <= n:
+            raise IndexError("partition index out of range")
+        lo = self.inf if i == 0 else self._points[i - 1]
+        hi = self.sup if i == n else self._points[i]
+        return RealInterval(lo, hi)
+
+    def intermediates(self):
+        return list(self._points)
+
+    def mesh(self):
+        """Length of the largest sub-interval."""
+        ends = [self.inf] + self._points + [self.sup]
+        return max(b - a for a, b in zip(ends[:-1], ends[1:]))
+
+    def refine_midpoints(self):
+        """The partition with the midpoint of every sub-interval added."""
+        ends = [self.inf] + self._points + [self.sup]
+        mids = [(a + b) / 2.0 for a, b in zip(ends[:-1], ends[1:])]
+        return Partition(RealInterval(self.inf, self.sup), self._points + mids)
 
 
 class DyadicInterval:
@@ -193,6 +234,44 @@ class _StreamQueries:
         a, b, res = self._interval_args(interval_or_inf, sup, resolution)
         sig = self._query(np.array([a]), np.array([b]), res, False, True)[1]
         return self._truncate_tensor(sig[0].cpu().numpy(), depth)
+
+    def restrict(self, interval):
+        """The same stream with its support replaced by ``interval``
+        (streams/src/stream.cpp:73-89, Stream::restrict): later queries are
+        trimmed to the new support, not to its intersection with the old
+        one.  The events are shared; a device tree is built again for the
+        new support on first use, since queries are trimmed where the tree
+        was built."""
+        inf, sup = ((interval.inf, interval.sup)
+                    if isinstance(interval, (RealInterval, DyadicInterval)) else interval)
+        new = copy.copy(self)
+        new._base_support = getattr(self, "_base_support", self.support)
+        new.support = RealInterval(float(inf), float(sup))
+        if hasattr(new, "_tree"):
+            new._tree = None
+        return new
+
+    def simplify(self, partition, resolution=None, ctx=None, depth=None):
+        """A PiecewiseAbelianStream with one piece per interval of
+        ``partition``: the interval's log-signature at ``resolution``
+        (default: the stream's) (streams/src/stream.cpp:232-258).  As in the
+        reference the new stream keeps the underlying stream's own support
+        (not one set by ``restrict``) and takes ``resolution`` as its
+        default; ``depth`` (or ``ctx.depth``) truncates the pieces."""
+        if not isinstance(partition, Partition):
+            partition = Partition(*partition)
+        if ctx is not None and depth is None:
+            depth = getattr(ctx, "depth", None)
+        res = self.resolution if resolution is None else int(resolution)
+        d = self.depth if not depth else min(int(depth), self.depth)
+        ivs = [partition[i] for i in range(len(partition))]
+        infs = np.array([iv.inf for iv in ivs])
+        sups = np.array([iv.sup for iv in ivs])
+        lies = self._query(infs, sups, res)[0].cpu().numpy()
+        lies = lies[:, :rpc.LieBasis(self.width, d).size()]
+        support = getattr(self, "_base_support", self.support)
+        return PiecewiseAbelianStream(infs, sups, lies, self.width, d, res,
+                                      RealInterval(support.inf, support.sup), self.device)
 
     def signature_derivative(self, interval, perturbation=None, resolution=None, depth=None):
         """Derivative of the signature along Lie perturbations

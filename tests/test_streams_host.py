@@ -240,3 +240,25 @@ def test_tick_stream_event_layout_for_the_tree():
         TickStream.from_lie_events([], np.zeros((0, 2)), 2, 2)
     with pytest.raises(NotImplementedError):
         TickStream.from_data({1.0: [("a", "increment", 1.0)]}, width=2, depth=2)
+
+
+def test_partition_and_restrict_host_side():
+    """Partition keeps the points strictly inside, sorted, duplicates
+    included (intervals/src/partition.cpp:45-56, :93-110); restrict replaces
+    the support without touching the events, and the restricted copy
+    rebuilds its device tree (nothing is built here)."""
+    from roughpy_b200.streams import LieIncrementStream, Partition, RealInterval
+    p = Partition(RealInterval(0.0, 1.0), [0.75, 0.25, 1.0, 0.0, 1.5, 0.25])
+    assert p.intermediates() == [0.25, 0.25, 0.75]
+    assert len(p) == 4
+    assert [(p[i].inf, p[i].sup) for i in range(4)] == [(0.0, 0.25), (0.25, 0.25), (0.25, 0.75),
+                                                       (0.75, 1.0)]
+    assert p.mesh() == 0.5
+    assert Partition((0.0, 1.0))[0].sup == 1.0
+    assert Partition((0.0, 1.0), [0.5]).refine_midpoints().intermediates() == [0.25, 0.5, 0.75]
+    st = LieIncrementStream.from_increments(np.ones((4, 2)), width=2, depth=2)
+    r = st.restrict(RealInterval(1.0, 2.5))
+    assert (r.support.inf, r.support.sup) == (1.0, 2.5)
+    assert (st.support.inf, st.support.sup) == (0.0, 4.0)
+    assert r._tree is None and r.lies is st.lies
+    assert r.restrict((0.0, 9.0))._base_support is st.support
