@@ -93,6 +93,14 @@ class Partition:
     def intermediates(self):
         return list(self._points)
 
+    def __eq__(self, other):
+        return (isinstance(other, Partition) and (self.inf, self.sup) == (other.inf, other.sup)
+                and self._points == other._points)
+
+    def __repr__(self):
+        ends = [self.inf] + self._points + [self.sup]
+        return "{" + ", ".join(f"[{a}, {b})" for a, b in zip(ends[:-1], ends[1:])) + "}"
+
     def mesh(self):
         """Length of the largest sub-interval."""
         ends = [self.inf] + self._points + [self.sup]

@@ -262,3 +262,15 @@ def test_partition_and_restrict_host_side():
     assert (st.support.inf, st.support.sup) == (0.0, 4.0)
     assert r._tree is None and r.lies is st.lies
     assert r.restrict((0.0, 9.0))._base_support is st.support
+
+
+def test_partition_reference_cases():
+    """tests/intervals/test_partitions.py:9-23: intermediates outside the
+    interval (or at its ends) are dropped; a pickle round trip compares
+    equal."""
+    import pickle
+    from roughpy_b200.streams import Partition, RealInterval
+    assert Partition(RealInterval(0.0, 1.0), intermediates=np.arange(10)).intermediates() == []
+    p = Partition(RealInterval(0.5, 1.6), [0.9, 1.3])
+    assert pickle.loads(pickle.dumps(p)) == p
+    assert p != Partition(RealInterval(0.5, 1.6), [0.9])
