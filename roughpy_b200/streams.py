@@ -154,6 +154,22 @@ def param_to_resolution(accuracy: float) -> int:
     return -min(5, e - 1)
 
 
+def _resolution_arg(resolution):
+    """A query's resolution argument as the bindings read it
+    (roughpy/src/streams/signature_arguments.cpp:30-50): None keeps the
+    default, an int is the resolution, a float is an accuracy turned into a
+    resolution by param_to_resolution."""
+    if resolution is None:
+        return None
+    if isinstance(resolution, (bool, np.bool_)):
+        raise TypeError("resolution should be either float or int")
+    if isinstance(resolution, (int, np.integer)):
+        return int(resolution)
+    if isinstance(resolution, (float, np.floating)):
+        return param_to_resolution(float(resolution))
+    raise TypeError("resolution should be either float or int")
+
+
 def _query_param_to_resolution(length: float) -> int:
     """streams/include/roughpy/streams/stream_base.h:74-83"""
     _, e = math.frexp(float(length))
@@ -184,18 +200,24 @@ class _StreamQueries:
 
     def _interval_args(self, interval_or_inf, sup, resolution=None):
         """(inf, sup, resolution): an interval, an inf/sup pair, nothing (the
-        whole support) or an integer alone (a resolution over the support)."""
+        whole support) or an integer alone (a resolution over the support).
+        After an interval the second argument is the resolution; a float
+        resolution is an accuracy (signature_arguments.cpp:30-50, :95-170)."""
         if interval_or_inf is None:
-            return self.support.inf, self.support.sup, resolution
+            return self.support.inf, self.support.sup, _resolution_arg(resolution)
         if isinstance(interval_or_inf, (RealInterval, DyadicInterval)):
-            return interval_or_inf.inf, interval_or_inf.sup, resolution
+            if sup is not None:
+                resolution = sup
+            return interval_or_inf.inf, interval_or_inf.sup, _resolution_arg(resolution)
         if sup is None:
             if isinstance(interval_or_inf, (int, np.integer)) and not isinstance(interval_or_inf, bool):
                 return self.support.inf, self.support.sup, int(interval_or_inf)
             raise TypeError("expecting integer resolution")
+        if not isinstance(sup, (int, float, np.integer, np.floating)) or isinstance(sup, bool):
+            raise TypeError("expected float value for sup")
         if float(interval_or_inf) > float(sup):
             raise ValueError("inf must not be larger than sup")
-        return float(interval_or_inf), float(sup), resolution
+        return float(interval_or_inf), float(sup), _resolution_arg(resolution)
 
     def _truncate_lie(self, lie, depth):
         if depth is None or depth >= self.depth:
@@ -209,6 +231,7 @@ class _StreamQueries:
 
     def log_signature_batch(self, infs, sups, resolution=None, chunk=16384):
         """Log-signatures (Hall coordinates, float64) of many clopen intervals."""
+        resolution = _resolution_arg(resolution)
         infs = np.asarray(infs, dtype=np.float64).reshape(-1)
         sups = np.asarray(sups, dtype=np.float64).reshape(-1)
         outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution)[0]
@@ -219,6 +242,7 @@ class _StreamQueries:
 
     def signature_batch(self, infs, sups, resolution=None, chunk=16384):
         """Signatures exp(l2t(log_signature)) (float64) of many clopen intervals."""
+        resolution = _resolution_arg(resolution)
         infs = np.asarray(infs, dtype=np.float64).reshape(-1)
         sups = np.asarray(sups, dtype=np.float64).reshape(-1)
         outs = [self._query(infs[i:i + chunk], sups[i:i + chunk], resolution, False, True)[1]
@@ -287,6 +311,7 @@ class _StreamQueries:
         ``perturbation`` (Hall coordinates), or a list of (interval,
         perturbation) pairs.  Each interval's log-signature comes from the
         stream's queries; float64 numpy tensor."""
+        resolution = _resolution_arg(resolution)
         pairs = list(interval) if perturbation is None else [(interval, perturbation)]
         ivs = [self._interval_args(iv, None) if isinstance(iv, (RealInterval, DyadicInterval))
                else self._interval_args(*iv) for iv, _ in pairs]

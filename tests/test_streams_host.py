@@ -274,3 +274,46 @@ def test_partition_reference_cases():
     p = Partition(RealInterval(0.5, 1.6), [0.9, 1.3])
     assert pickle.loads(pickle.dumps(p)) == p
     assert p != Partition(RealInterval(0.5, 1.6), [0.9])
+
+
+def test_query_argument_rules():
+    """signature_arguments.cpp:30-50 and :95-170: a float resolution is an
+    accuracy (param_to_resolution), after an interval the second argument is
+    the resolution, a float alone is rejected, and sup must be a number."""
+    from roughpy_b200.streams import (LieIncrementStream, RealInterval, _resolution_arg,
+                                      param_to_resolution)
+    assert _resolution_arg(None) is None
+    assert _resolution_arg(3) == 3 and _resolution_arg(np.int32(4)) == 4
+    assert _resolution_arg(0.5) == param_to_resolution(0.5) == 1
+    assert _resolution_arg(0.25) == 2 and _resolution_arg(np.float64(1e-3)) == 10
+    assert _resolution_arg(100.0) == -5   # coarse accuracies stop at resolution -5
+    with pytest.raises(TypeError):
+        _resolution_arg("4")
+    with pytest.raises(TypeError):
+        _resolution_arg(True)
+    st = LieIncrementStream.from_increments(np.ones((4, 2)), width=2, depth=2)
+    assert st._interval_args(RealInterval(0.0, 1.0), 3) == (0.0, 1.0, 3)
+    assert st._interval_args(RealInterval(0.0, 1.0), 0.25) == (0.0, 1.0, 2)
+    assert st._interval_args(0.0, 0.8, 0.5) == (0.0, 0.8, 1)
+    assert st._interval_args(5, None) == (0.0, 4.0, 5)
+    assert st._interval_args(None, None, 0.125) == (0.0, 4.0, 3)
+    with pytest.raises(TypeError):
+        st._interval_args(0.5, None)
+    with pytest.raises(TypeError):
+        st._interval_args(0.0, "1")
+    with pytest.raises(ValueError):
+        st._interval_args(1.0, 0.0)
+
+
+def test_restated_stream_accuracy_arguments(golden):
+    """tests/streams/test_lie_increment_path.py:132-143: one tick at 0.7;
+    accuracy 0.5 (resolution 1) sees nothing in [0, 0.8), accuracy 0.25
+    (resolution 2) sees the tick."""
+    from roughpy_b200.streams import param_to_resolution
+    a = arith(golden, 2, 2)
+    st = R.StreamRef(a, np.array([[1.0, 2.5]]), indices=np.array([0.7]))
+    unit = np.zeros(a.T)
+    unit[0] = 1.0
+    np.testing.assert_array_equal(st.signature(0.0, 0.8, param_to_resolution(0.5)), unit)
+    np.testing.assert_allclose(st.signature(0.0, 0.8, param_to_resolution(0.25)),
+                               [1.0, 1.0, 2.5, 0.5, 1.25, 1.25, 3.125], atol=1e-15)
