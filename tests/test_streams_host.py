@@ -317,3 +317,54 @@ def test_restated_stream_accuracy_arguments(golden):
     np.testing.assert_array_equal(st.signature(0.0, 0.8, param_to_resolution(0.5)), unit)
     np.testing.assert_allclose(st.signature(0.0, 0.8, param_to_resolution(0.25)),
                                [1.0, 1.0, 2.5, 0.5, 1.25, 1.25, 3.125], atol=1e-15)
+
+
+def _straight_line_signature(w, d, length):
+    """The signature of a straight line with increment length * (1, ..., w):
+    level k holds prod(word) * length^k / k! (tests/streams/
+    test_lie_increment_path.py:171-195, solution_signature)."""
+    import itertools
+    out = [1.0]
+    for k in range(1, d + 1):
+        for word in itertools.product(range(1, w + 1), repeat=k):
+            out.append(float(np.prod(word)) * length ** k / math.factorial(k))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("w,d", [(2, 2), (2, 4), (3, 3), (4, 3)])
+@pytest.mark.parametrize("n", [2, 5, 10, 25, 100])
+def test_restated_stream_known_straight_line_signature(golden, w, d, n):
+    """tests/streams/test_lie_increment_path.py:160-205: n equal increments
+    2/n * (1, ..., w) at t = 2/n, 4/n, ..., 2; the signature over [0, 3.125)
+    is that of the straight line over [0, 2]."""
+    a = arith(golden, w, d)
+    t_values = np.arange(0.0, 2.0, 2.0 / n) + 2.0 / n
+    data = np.tensordot(np.ones(n), np.arange(1.0, w + 1) * (2.0 / n), axes=0)
+    st = R.StreamRef(a, data, indices=t_values)
+    np.testing.assert_allclose(st.signature(0.0, 3.125), _straight_line_signature(w, d, 2.0),
+                               rtol=1e-12, atol=1e-12)
+
+
+def test_restated_stream_signature_multiplication(golden):
+    """tests/streams/test_lie_increment_path.py:386-399 (float64 here):
+    the signatures over [0, pi/4) and [pi/4, 2) multiply to the one over
+    [0, 2)."""
+    import oracle
+    a = arith(golden, 3, 2)
+    data = np.array([[0., 1., 2.], [3., 4., 5.], [6., 7., 8.]])
+    st = R.StreamRef(a, data, indices=np.array([0., np.pi / 4, 1.0]))
+    left = st.signature(0.0, np.pi / 4)
+    right = st.signature(np.pi / 4, 2.0)
+    full = st.signature(0.0, 2.0)
+    np.testing.assert_allclose(oracle.ft_mul(3, 2, left, right), full, rtol=1e-12, atol=1e-12)
+
+
+def test_restated_stream_of_lie_elements(golden):
+    """tests/streams/test_lie_increment_path.py:401-413: a sequence of Lie
+    elements at t = 0, 1, 2; the log-signature over [0, 1) is the first."""
+    a = arith(golden, 3, 3)
+    seq = np.array([[1., 2., 3.], [4., 5., 6.], [7., 8., 9.]])
+    st = R.StreamRef(a, seq)
+    lie = st.log_signature(0.0, 1.0)
+    np.testing.assert_array_equal(lie[:3], seq[0])
+    assert not np.any(lie[3:])
