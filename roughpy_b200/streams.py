@@ -525,6 +525,12 @@ class TickStream(LieIncrementStream):
         return cls(starts, lies[order], width, depth, res, support, dtype, mode, device)
 
     @classmethod
+    def from_increments(cls, *args, **kwargs):
+        # LieIncrementStream's constructor de-duplicates event times, which a
+        # tick stream does not
+        raise TypeError("a TickStream is built with TickStream.from_lie_events")
+
+    @classmethod
     def from_data(cls, *args, **kwargs):
         raise NotImplementedError(
             "tick data parsing (labels, channel types, schemas) is not provided; build the "

@@ -240,6 +240,8 @@ def test_tick_stream_event_layout_for_the_tree():
         TickStream.from_lie_events([], np.zeros((0, 2)), 2, 2)
     with pytest.raises(NotImplementedError):
         TickStream.from_data({1.0: [("a", "increment", 1.0)]}, width=2, depth=2)
+    with pytest.raises(TypeError):
+        TickStream.from_increments(rows, width=2, depth=2)
 
 
 def test_partition_and_restrict_host_side():
