@@ -68,6 +68,18 @@ def test_version_and_sizes():
     lambda L: L.rpyb_sig_derivative(3, 3, 3, 1, None, None, None, 6, None, 40, None, 0, None),
     lambda L: L.rpyb_sig_derivative(1, 3, 3, 1, (ctypes.c_int64 * 2)(1, 2), None, None, 14, 8,
                                     40, None, 0, None),
+    # sparse map: bad dtype, negative size, null CSR, row stride below the size
+    lambda L: L.rpyb_sparse_map(7, 4, 4, 1, 8, 8, 8, 8, 8, 4, 4, 1.0, None),
+    lambda L: L.rpyb_sparse_map(1, -1, 4, 1, 8, 8, 8, 8, 8, 4, 4, 1.0, None),
+    lambda L: L.rpyb_sparse_map(1, 4, 4, 2, None, None, None, 8, 8, 4, 4, 1.0, None),
+    lambda L: L.rpyb_sparse_map(1, 4, 4, 2, 8, 8, 8, 8, 8, 3, 4, 1.0, None),
+    # tensor <-> Lie maps at (3,3) (L = 14, T = 40): bad dtype, negative batch,
+    # null rows, strides below the sizes
+    lambda L: L.rpyb_tensor_to_lie(7, 3, 3, 1, 8, 14, 8, 40, None),
+    lambda L: L.rpyb_tensor_to_lie(1, 3, 3, -1, 8, 14, 8, 40, None),
+    lambda L: L.rpyb_tensor_to_lie(1, 3, 3, 2, None, 14, 8, 40, None),
+    lambda L: L.rpyb_tensor_to_lie(1, 3, 3, 2, 8, 13, 8, 40, None),
+    lambda L: L.rpyb_lie_to_tensor(1, 3, 3, 2, 8, 39, 8, 14, None),
 ])
 def test_invalid_arguments_are_rejected_before_any_launch(call):
     from roughpy_b200 import _lib
@@ -82,6 +94,9 @@ def test_zero_batch_is_a_no_op():
     assert _lib.lib.rpyb_signature(1, 2, 2, 0, None, None, None, 7, None, None, 0, None) == 0
     assert _lib.lib.rpyb_sig_derivative(1, 3, 3, 0, None, None, None, 14, None, 40, None, 0,
                                         None) == 0
+    assert _lib.lib.rpyb_sparse_map(1, 4, 4, 0, None, None, None, None, None, 4, 4, 1.0,
+                                    None) == 0
+    assert _lib.lib.rpyb_tensor_to_lie(1, 3, 3, 0, None, 14, None, 40, None) == 0
     assert _lib.lib.rpyb_dyadic_free(None) == 0
     assert _lib.lib.rpyb_release_cached_memory() == 0
 
