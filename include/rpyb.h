@@ -225,6 +225,63 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
                             void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * rpyb_signature with an accuracy report.  err_out (device float64
+ * [n_streams], nullable) receives, per stream, the largest per-level relative
+ * error max_k ||out_k - ref_k||_inf / ||ref_k||_inf of the result against the
+ * float64 GPU path run on the same increments in the same launch layout (the
+ * absolute error for a level whose reference is zero).  For RPYB_F64 the
+ * result is its own reference and err_out is zeroed.  total_rows =
+ * offsets[n_streams] (the host value; it sizes the float64 copy of the
+ * increments).  The report costs one float64 launch besides the float32 one;
+ * its workspace holds the float64 signatures ([n_streams, tensor_size]) and
+ * increments.  err_out == NULL is rpyb_signature.
+ * Replaces: the same reference path as rpyb_signature; the report is the
+ * per-result accuracy statement of the float32 mode (the reference computes
+ * in float64 only).
+ */
+RPYB_API int64_t rpyb_signature_batched_workspace_size(int mode, int32_t width, int32_t depth,
+                                                       int64_t n_streams, int64_t total_rows,
+                                                       int with_error);
+RPYB_API int rpyb_signature_batched(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                                    const int64_t* offsets, const void* increments,
+                                    int64_t total_rows, void* out, int64_t ld_out,
+                                    const int64_t* order, double* err_out, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+
+/*
+ * Signature plans: a batch layout whose stream lengths are known on the host
+ * (offsets_host, n_streams + 1 entries), with its launch schedule and device
+ * tables, reused across calls.  A schedule sets the kernel's lane shape (the
+ * level split: level-(N-1) words per lane), the warps per block and a time-
+ * segment length: streams longer than it are cut into balanced segments that
+ * run as separate work items of the persistent launch, and the segment
+ * signatures are multiplied back in order by a pairwise tree of batched
+ * products (the Chen product is associative), so a few very long streams
+ * still fill the GPU.  The schedule comes from RPYB_SIG_SCHEDULE
+ * ("g=8,wpb=0,seg=4096"), else from the JSON cache at RPYB_SIG_TUNE_CACHE
+ * (default $XDG_CACHE_HOME/roughpy_b200/signature_schedules.json) keyed on
+ * (device, mode, width, depth, log2 longest stream, log2 batch size), else,
+ * with flags & RPYB_SIG_PLAN_TUNE, by timing the candidates on synthetic
+ * increments of this layout on `stream` (then cached); otherwise the
+ * defaults.  Creation allocates the plan's device memory and waits for
+ * `stream`; rpyb_sig_plan_run allocates nothing (except the float64 buffers
+ * of the first call with err_out, see rpyb_signature_batched).  One run at a
+ * time per plan.  rpyb_sig_plan_describe writes a JSON description of the
+ * schedule into buf (cap bytes) and returns its length.
+ * Replaces: algebra/src/lite_context.h:542-563 (compute_signature) for a
+ *           batch, like rpyb_signature.
+ */
+typedef struct rpyb_sig_plan rpyb_sig_plan;
+#define RPYB_SIG_PLAN_TUNE 1
+RPYB_API int rpyb_sig_plan_create(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                                  const int64_t* offsets_host, int32_t flags, void* stream,
+                                  rpyb_sig_plan** plan);
+RPYB_API int rpyb_sig_plan_run(rpyb_sig_plan* plan, const void* increments, void* out,
+                               int64_t ld_out, double* err_out, void* stream);
+RPYB_API int rpyb_sig_plan_describe(const rpyb_sig_plan* plan, char* buf, int64_t cap);
+RPYB_API int rpyb_sig_plan_free(rpyb_sig_plan* plan);
+
+/*
  * rpyb_signature from host memory, end to end: increments [total, width] and
  * the output [n_streams, ld_out] are HOST buffers (pin them for overlap),
  * offsets_host is a host int64 array.  The streams are processed in n_chunks
@@ -253,9 +310,13 @@ RPYB_API int rpyb_signature_host(int mode, int32_t width, int32_t depth, int64_t
  * increment gradients; states are recovered by inverse steps re-anchored on
  * float64 checkpoints every `checkpoint_every` steps (widths 2..8 with
  * width^(depth-2) <= 992), or recomputed per segment from them (other
- * shapes).  Adjoint accumulators are float64 in both modes.  `max_len` must
- * bound every stream length (it sizes the checkpoint scratch); longer streams
- * get NaN gradients.  Width <= 8.
+ * shapes).  Adjoint accumulators are float64 in both modes.  `max_len` sizes
+ * the checkpoint scratch and must bound every stream length; -1 takes the
+ * longest stream.  Before launching, the call reduces the offsets on the
+ * device and reads the longest and shortest length back (a 16-byte read that
+ * waits for `stream`; the call is therefore not capturable in a CUDA graph):
+ * a stream longer than max_len, or decreasing offsets, fail with
+ * RPYB_E_INVALID and nothing is written.  Width <= 8.
  * No reference counterpart: RoughPy only has the forward-mode derivative
  * (algebra/src/lite_context.h:577-636, LiteContext::sig_derivative_impl).
  */

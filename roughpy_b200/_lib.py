@@ -69,6 +69,13 @@ SIGNATURES = {
                                         _pi32, _vp]),
     "rpyb_signature_workspace_size": (_i64, [_int, _i32, _i32, _i64]),
     "rpyb_signature": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "rpyb_signature_batched_workspace_size": (_i64, [_int, _i32, _i32, _i64, _i64, _int]),
+    "rpyb_signature_batched": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _i64, _vp, _i64, _vp,
+                                      _vp, _vp, _sz, _vp]),
+    "rpyb_sig_plan_create": (_int, [_int, _i32, _i32, _i64, _vp, _i32, _vp, _vp]),
+    "rpyb_sig_plan_run": (_int, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "rpyb_sig_plan_describe": (_int, [_vp, ctypes.c_char_p, _i64]),
+    "rpyb_sig_plan_free": (_int, [_vp]),
     "rpyb_signature_host_device_bytes": (_i64, [_int, _i32, _i32, _i64, _vp, _i32]),
     "rpyb_signature_host": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i32, _vp, _sz,
                                    _vp]),
@@ -96,6 +103,9 @@ SIGNATURES = {
     "rpyb_sig_derivative": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
                                    _sz, _vp]),
 }
+
+# rpyb_sig_plan_create flag: time the schedule candidates when no cached choice exists
+SIG_PLAN_TUNE = 1
 
 # rpyb_dyadic_query: choose the dissection resolution per query as the reference does
 QUERY_RESOLUTION_AUTO = -2147483648

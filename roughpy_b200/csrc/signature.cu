@@ -31,18 +31,28 @@
 // width 8 its hi words too) live in shared memory: they are touched only
 // when folding, which leaves the registers to the delta accumulators.
 #include <algorithm>
+#include <initializer_list>
 #include <mutex>
 #include <tuple>
 #include <map>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
+#include "signature_internal.cuh"
 
 namespace rpyb {
 namespace {
 
 constexpr int kSigWarps = 8;  // warps per block of the persistent kernel
 constexpr int kChunk = 32;    // increment rows staged per warp in shared memory
+
+// register cap of the float32 split kernel: without it the compiler hoists
+// the fold's shared-memory loads and uses over 230 registers at width 8;
+// 192 fits ten warps per SM (the shared-memory limit at width 8) unspilled
+#ifndef RPYB_SIG_SPLIT_MAXREG
+#define RPYB_SIG_SPLIT_MAXREG 192
+#endif
 
 // level-(N-1) words per lane of the float64 kernel at width 8
 #ifndef RPYB_SIG_F64_G8
@@ -60,8 +70,22 @@ struct SigArgs {
     int64_t total_items;
     int* queue;   // device work counter (zeroed before launch)
     int fold;     // fold interval of the compensated mode (steps)
+    // output rows: row s of `out` unless dst_row is given, in which case
+    // r = dst_row[s] selects row r of `out` (r >= 0) or row ~r of `alt`
+    // (r < 0; the segment rows of split streams)
+    const int64_t* dst_row;
+    void* alt;
+    int64_t ld_alt;
     int64_t db[kMaxDepth + 2];
 };
+
+template <typename T>
+__device__ __forceinline__ T* output_row(const SigArgs& a, int64_t s)
+{
+    if (a.dst_row == nullptr) return static_cast<T*>(a.out) + s * a.ld_out;
+    const int64_t r = a.dst_row[s];
+    return r >= 0 ? static_cast<T*>(a.out) + r * a.ld_out : static_cast<T*>(a.alt) + (~r) * a.ld_alt;
+}
 
 template <int D, int E>
 struct IPow {
@@ -412,7 +436,7 @@ signature_kernel(const SigArgs a)
 
         // ---- write the stream's words owned by this lane
         if (active) {
-            T* __restrict__ o = static_cast<T*>(a.out) + s * a.ld_out;
+            T* __restrict__ o = output_row<T>(a, s);
             if (beta == 0) o[0] = T(1);
             // path words: owned by the lane whose remaining digits are zero
             {
@@ -452,6 +476,267 @@ signature_kernel(const SigArgs a)
                     } else tv = th[g][b] + (lo_top[(g * D + b) * 32 + lane] + td[g][b]);
                     o[a.db[N] + mw * D + b] = tv;
                 }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------
+// float32 mode on both arithmetic pipes ("split" kernel).
+//
+// The classic float32 kernel above spends a third of its FP32 pipe on work
+// that is not a top-level product: the Horner chains through the path words,
+// the path updates, the `hi + delta` reads and the folds.  B200 issues FP64
+// instructions to a pipe of their own, so this kernel moves all of that to
+// float64 and leaves the FP32 pipe only the products that carry the bulk of
+// the work:
+//   * path words (levels 1..N-2) are float64 registers updated with DFMAs,
+//     and both Horner chains run in float64 from float64 copies of the staged
+//     increments; each chain ends in one conversion to float32;
+//   * the G mid words (level N-1) keep a float32 delta `md` for the current
+//     chunk of kChunk steps and a float64 value in shared memory;
+//   * the G*D top words keep a float32 delta `td` per chunk and a float64
+//     value in shared memory.
+// Within a chunk the top word (w, b) grows by sum_t am_t[w] x_t[b] with
+// am_t = S_{N-1}[w] + chain_t * x_t[w]/2, and S_{N-1}[w] = m64 + md_t where
+// m64 is the mid word's float64 value at the start of the chunk.  So
+//   sum_t am_t x_t[b] = m64 * X[b] + sum_t (md_t + chain_t x_t[w]/2) x_t[b],
+// X being the chunk's increment sum: the per-step float32 work is the small
+// residual r_t = fma(chain_t/2, x_t[w], md_t) and the products r_t x_t[b]
+// (FFMA2), while m64 * X[b] is added in float64 when the chunk's deltas are
+// folded (one DFMA per word per chunk).  Per step and lane the FP32 pipe sees
+// G*D + 2G FMAs, every one of them a useful Horner FMA.
+template <int D, int N, int G>
+__global__ void __maxnreg__(RPYB_SIG_SPLIT_MAXREG)
+signature_kernel_split(const SigArgs a)
+{
+    constexpr int P = N - 2;                 // path levels 1..N-2
+    constexpr int PP = P > 0 ? P : 1;
+    constexpr int SUBS = D / G;              // lanes sharing one level-(N-2) word
+    constexpr int64_t W = IPow<D, (P > 0 ? P : 0)>::value * SUBS;  // lanes per stream
+    constexpr int TOPW = G * D;              // top words per lane
+    static_assert(D % G == 0, "G must divide D");
+    constexpr bool PACK_T = (D % 2 == 0);    // top words in f32x2 pairs
+    constexpr bool PACK_M = (G % 2 == 0);    // mid words in f32x2 pairs
+
+    // dynamic shared memory per warp: top values [TOPW][32] f64, mid values
+    // [G][32] f64, chunk sums [D] f64 (16-byte padded), staged rows
+    // [kChunk][D] f64 then [kChunk][D] f32
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    constexpr size_t kXsumBytes = ((size_t)D * 8 + 15) / 16 * 16;
+    constexpr size_t kWarpBytes = (size_t)(TOPW + G) * 32 * 8 + kXsumBytes +
+                                  (size_t)kChunk * D * 12;
+    unsigned char* wbase = smem_raw + (size_t)warp * kWarpBytes;
+    double* top64 = reinterpret_cast<double*>(wbase);
+    double* mid64 = top64 + TOPW * 32;
+    double* xsum = mid64 + G * 32;
+    double* x64 = reinterpret_cast<double*>(wbase + (size_t)(TOPW + G) * 32 * 8 + kXsumBytes);
+    float* x32 = reinterpret_cast<float*>(x64 + kChunk * D);
+
+    while (true) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.total_items) break;
+
+        const int64_t slot = item / a.items_per_stream;
+        const int64_t blk = item - slot * a.items_per_stream;
+        const int64_t s = a.order ? a.order[slot] : slot;
+        const int64_t beta_raw = blk * 32 + lane;
+        const bool active = beta_raw < W;
+        const int64_t beta = active ? beta_raw : (W - 1);
+        const int64_t pi = beta / SUBS;
+        const int sub = (int)(beta - pi * SUBS);
+
+        int c[PP];
+        {
+            int64_t t = pi;
+#pragma unroll
+            for (int i = P - 1; i >= 0; --i) {
+                c[i] = (int)(t % D);
+                t /= D;
+            }
+        }
+
+        const int64_t start = a.offsets[s];
+        const int64_t len = a.offsets[s + 1] - start;
+        const float* __restrict__ xs = static_cast<const float*>(a.inc) + start * D;
+
+        double ph[PP];
+        float md[G], td[G][D];
+#pragma unroll
+        for (int i = 0; i < PP; ++i) ph[i] = 0.0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            md[g] = 0.f;
+#pragma unroll
+            for (int b = 0; b < D; ++b) td[g][b] = 0.f;
+        }
+#pragma unroll 4
+        for (int w = 0; w < TOPW + G; ++w) top64[w * 32 + lane] = 0.0;
+
+        float nx[D];
+        if (lane < len) load_row<float, D>(nx, xs + (int64_t)lane * D);
+        for (int64_t t0 = 0; t0 < len; t0 += kChunk) {
+            const int nsteps = (int)min((int64_t)kChunk, len - t0);
+            __syncwarp();
+            // stage row t0 + lane in both precisions
+            if (lane < nsteps) {
+                store_row<float, D>(x32 + lane * D, nx);
+                double xd[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) xd[i] = (double)nx[i];
+                store_row<double, D>(x64 + lane * D, xd);
+            }
+            __syncwarp();
+            if (t0 + kChunk + lane < len) load_row<float, D>(nx, xs + (t0 + kChunk + lane) * D);
+
+#pragma unroll 1
+            for (int j = 0; j < nsteps; ++j) {
+                const float* row = x32 + j * D;
+                const double* row64 = x64 + j * D;
+                float x[D];
+                load_row_smem<float, D>(x, row);
+                float xa[G];
+                if constexpr (SUBS == 1) {
+#pragma unroll
+                    for (int g = 0; g < G; ++g) xa[g] = x[g];
+                } else {
+                    load_slice<float, G>(xa, row + sub * G);
+                }
+                double xc[PP];
+#pragma unroll
+                for (int i = 0; i < P; ++i) xc[i] = row64[c[i]];
+
+                // ---- top level: chain through the path (f64), residual and
+                // products (f32)
+                float accx = 0.5f;
+                if constexpr (P > 0) {
+                    double acc = fma(xc[0], 1.0 / N, ph[0]);
+#pragma unroll
+                    for (int i = 2; i <= P; ++i) acc = fma(acc, xc[i - 1] * (1.0 / (N - i + 1)), ph[i - 1]);
+                    accx = (float)(acc * 0.5);
+                }
+                float r[G];
+                if constexpr (PACK_M) {
+#pragma unroll
+                    for (int g = 0; g < G; g += 2) {
+                        const float2 q = __ffma2_rn(make_float2(accx, accx), make_float2(xa[g], xa[g + 1]),
+                                                    make_float2(md[g], md[g + 1]));
+                        r[g] = q.x;
+                        r[g + 1] = q.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int g = 0; g < G; ++g) r[g] = fmaf(accx, xa[g], md[g]);
+                }
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    if constexpr (PACK_T) {
+                        const float2 r2 = make_float2(r[g], r[g]);
+#pragma unroll
+                        for (int h = 0; h < D / 2; ++h) {
+                            const float2 q = __ffma2_rn(r2, make_float2(x[2 * h], x[2 * h + 1]),
+                                                        make_float2(td[g][2 * h], td[g][2 * h + 1]));
+                            td[g][2 * h] = q.x;
+                            td[g][2 * h + 1] = q.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < D; ++b) td[g][b] = fmaf(r[g], x[b], td[g][b]);
+                    }
+                }
+                // ---- level N-1: chain (f64), deltas (f32)
+                float accm = 1.f;
+                if constexpr (P > 0) {
+                    double acc = fma(xc[0], 1.0 / (N - 1), ph[0]);
+#pragma unroll
+                    for (int i = 2; i <= P; ++i) acc = fma(acc, xc[i - 1] * (1.0 / (N - i)), ph[i - 1]);
+                    accm = (float)acc;
+                }
+                if constexpr (PACK_M) {
+#pragma unroll
+                    for (int g = 0; g < G; g += 2) {
+                        const float2 q = __ffma2_rn(make_float2(accm, accm), make_float2(xa[g], xa[g + 1]),
+                                                    make_float2(md[g], md[g + 1]));
+                        md[g] = q.x;
+                        md[g + 1] = q.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int g = 0; g < G; ++g) md[g] = fmaf(accm, xa[g], md[g]);
+                }
+                // ---- path levels k = P .. 1 (f64)
+#pragma unroll
+                for (int k = P; k >= 1; --k) {
+                    if (k == 1) {
+                        ph[0] += xc[0];
+                    } else {
+                        double acc = fma(xc[0], 1.0 / k, ph[0]);
+#pragma unroll
+                        for (int i = 2; i <= k - 1; ++i) acc = fma(acc, xc[i - 1] * (1.0 / (k - i + 1)), ph[i - 1]);
+                        ph[k - 1] = fma(acc, xc[k - 1], ph[k - 1]);
+                    }
+                }
+            }
+
+            // ---- fold the chunk: top += m64 * X + td, mid += md (float64)
+            if (lane < D) {
+                double sum = 0.0;
+                for (int j = 0; j < nsteps; ++j) sum += x64[j * D + lane];
+                xsum[lane] = sum;
+            }
+            __syncwarp();
+            double X[D];
+            load_row_smem<double, D>(X, xsum);
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                double* mp = mid64 + g * 32 + lane;
+                const double m = *mp;
+#pragma unroll
+                for (int b = 0; b < D; ++b) {
+                    double* tp = top64 + (g * D + b) * 32 + lane;
+                    *tp = fma(m, X[b], *tp + (double)td[g][b]);
+                    td[g][b] = 0.f;
+                }
+                *mp = m + (double)md[g];
+                md[g] = 0.f;
+            }
+        }
+
+        // ---- write the stream's words owned by this lane
+        if (active) {
+            float* __restrict__ o = output_row<float>(a, s);
+            if (beta == 0) o[0] = 1.f;
+            {
+                bool zero_below = (sub == 0);
+                int64_t prefix = pi;
+#pragma unroll
+                for (int k = P; k >= 1; --k) {
+                    if (zero_below) o[a.db[k] + prefix] = (float)ph[k - 1];
+                    zero_below = zero_below && (c[k - 1] == 0);
+                    prefix /= D;
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int64_t mw = pi * D + sub * G + g;
+                o[a.db[N - 1] + mw] = (float)mid64[g * 32 + lane];
+                float tv[D];
+#pragma unroll
+                for (int b = 0; b < D; ++b) tv[b] = (float)top64[(g * D + b) * 32 + lane];
+                if constexpr (D % 4 == 0) {
+                    // a lane's D top words below one mid word are contiguous
+                    float* dst = o + a.db[N] + mw * D;
+                    if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                        store_row<float, D>(dst, tv);
+                        continue;
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < D; ++b) o[a.db[N] + mw * D + b] = tv[b];
             }
         }
     }
@@ -516,16 +801,25 @@ struct SigVariant {
     SigKernel fn;
     int g;
     int64_t lanes;          // W: lanes per stream
-    int top_words;          // G * D
-    int top_smem_floats;    // per warp, top-level words kept in shared memory
+    size_t smem_warp;       // dynamic shared memory per warp (bytes)
 };
 
 template <bool F64, int D, int N, int G, bool HS>
 SigVariant make_variant()
 {
     constexpr int64_t W = IPow<D, N - 2>::value * (D / G);
-    constexpr int smem = F64 ? 0 : (HS ? 2 : 1) * G * D * 32;
-    return SigVariant{&signature_kernel<F64, D, N, G, HS>, G, W, G * D, smem};
+    constexpr size_t top = F64 ? 0 : (size_t)(HS ? 2 : 1) * G * D * 32 * 4;
+    constexpr size_t stage = (size_t)kChunk * D * (F64 ? 8 : 4);
+    return SigVariant{&signature_kernel<F64, D, N, G, HS>, G, W, top + stage};
+}
+
+template <int D, int N, int G>
+SigVariant make_split_variant()
+{
+    constexpr int64_t W = IPow<D, N - 2>::value * (D / G);
+    constexpr size_t xsum = ((size_t)D * 8 + 15) / 16 * 16;
+    constexpr size_t bytes = (size_t)(G * D + G) * 32 * 8 + xsum + (size_t)kChunk * D * 12;
+    return SigVariant{&signature_kernel_split<D, N, G>, G, W, bytes};
 }
 
 template <bool F64, int D, int G, bool HS>
@@ -547,23 +841,206 @@ bool pick_depth(int n, SigVariant& v)
     }
 }
 
-// Lane shapes per width: G level-(N-1) words (and G*D top words) per lane.
-// float mode at width 8 keeps the top-level hi words in shared memory so that
-// a lane can own all 64 top words below one level-(N-2) word.
-template <bool F64>
-bool pick_variant(int d, int n, SigVariant& v)
+template <int D, int G>
+bool pick_split_depth(int n, SigVariant& v)
 {
-    switch (d) {
-        case 2: return pick_depth<F64, 2, 2, false>(n, v);
-        case 3: return pick_depth<F64, 3, 3, false>(n, v);
-        case 4: return pick_depth<F64, 4, 4, false>(n, v);
-        case 5: return pick_depth<F64, 5, 5, false>(n, v);
-        case 6: return pick_depth<F64, 6, 3, false>(n, v);
-        case 7: return pick_depth<F64, 7, 7, false>(n, v);
+    switch (n) {
+        case 2: v = make_split_variant<D, 2, G>(); return true;
+        case 3: v = make_split_variant<D, 3, G>(); return true;
+        case 4: v = make_split_variant<D, 4, G>(); return true;
+        case 5: v = make_split_variant<D, 5, G>(); return true;
+        case 6: v = make_split_variant<D, 6, G>(); return true;
+        case 7:
+            if constexpr (D <= 4) { v = make_split_variant<D, 7, G>(); return true; }
+            return false;
         case 8:
-            if constexpr (F64) return pick_depth<F64, 8, RPYB_SIG_F64_G8, false>(n, v);
-            else return pick_depth<F64, 8, 8, true>(n, v);
+            if constexpr (D <= 3) { v = make_split_variant<D, 8, G>(); return true; }
+            return false;
         default: return false;
+    }
+}
+
+// Kernel families of the specialised path.
+enum SigFamily { kFamilyClassic = 0, kFamilySplit = 1 };
+
+// Lane shapes: G level-(N-1) words (and G*D top words) per lane.  The first
+// entry of each list is the default; the others are the autotuner's
+// alternatives.  G only decides how a stream's words are dealt to lanes:
+// every word sees the same arithmetic whatever G is, so the alternatives
+// give bitwise identical results.
+//  - float64: G words of double state per lane;
+//  - classic float32: at width 8 the top-level hi words live in shared
+//    memory so that one lane can own all 64 top words below its word;
+//  - split float32: G*D float32 deltas per lane.
+bool lane_shapes(int mode, int family, int d, int* gs, int* count)
+{
+    *count = 0;
+    auto put = [&](std::initializer_list<int> l) { for (int g : l) gs[(*count)++] = g; };
+    if (mode == RPYB_F64) {
+        switch (d) {
+            case 2: put({2}); break;
+            case 3: put({3}); break;
+            case 4: put({4, 2}); break;
+            case 5: put({5}); break;
+            case 6: put({3, 6}); break;
+            case 7: put({7}); break;
+            case 8: put({RPYB_SIG_F64_G8, RPYB_SIG_F64_G8 == 8 ? 4 : 8}); break;
+            default: return false;
+        }
+    } else if (family == kFamilyClassic) {
+        switch (d) {
+            case 2: put({2}); break;
+            case 3: put({3}); break;
+            case 4: put({4}); break;
+            case 5: put({5}); break;
+            case 6: put({3}); break;
+            case 7: put({7}); break;
+            case 8: put({8}); break;
+            default: return false;
+        }
+    } else {
+        switch (d) {
+            case 2: put({2}); break;
+            case 3: put({3}); break;
+            case 4: put({4, 2}); break;
+            case 5: put({5}); break;
+            case 6: put({6, 3}); break;
+            case 7: put({7}); break;
+            case 8: put({8, 4}); break;
+            default: return false;
+        }
+    }
+    return true;
+}
+
+bool pick_f64(int d, int n, int g, SigVariant& v)
+{
+    switch (d * 16 + g) {
+        case 2 * 16 + 2: return pick_depth<true, 2, 2, false>(n, v);
+        case 3 * 16 + 3: return pick_depth<true, 3, 3, false>(n, v);
+        case 4 * 16 + 4: return pick_depth<true, 4, 4, false>(n, v);
+        case 4 * 16 + 2: return pick_depth<true, 4, 2, false>(n, v);
+        case 5 * 16 + 5: return pick_depth<true, 5, 5, false>(n, v);
+        case 6 * 16 + 3: return pick_depth<true, 6, 3, false>(n, v);
+        case 6 * 16 + 6: return pick_depth<true, 6, 6, false>(n, v);
+        case 7 * 16 + 7: return pick_depth<true, 7, 7, false>(n, v);
+        case 8 * 16 + 8: return pick_depth<true, 8, 8, false>(n, v);
+        case 8 * 16 + 4: return pick_depth<true, 8, 4, false>(n, v);
+        default: return false;
+    }
+}
+
+bool pick_classic_f32(int d, int n, int g, SigVariant& v)
+{
+    switch (d * 16 + g) {
+        case 2 * 16 + 2: return pick_depth<false, 2, 2, false>(n, v);
+        case 3 * 16 + 3: return pick_depth<false, 3, 3, false>(n, v);
+        case 4 * 16 + 4: return pick_depth<false, 4, 4, false>(n, v);
+        case 5 * 16 + 5: return pick_depth<false, 5, 5, false>(n, v);
+        case 6 * 16 + 3: return pick_depth<false, 6, 3, false>(n, v);
+        case 7 * 16 + 7: return pick_depth<false, 7, 7, false>(n, v);
+        case 8 * 16 + 8: return pick_depth<false, 8, 8, true>(n, v);
+        default: return false;
+    }
+}
+
+bool pick_split(int d, int n, int g, SigVariant& v)
+{
+    switch (d * 16 + g) {
+        case 2 * 16 + 2: return pick_split_depth<2, 2>(n, v);
+        case 3 * 16 + 3: return pick_split_depth<3, 3>(n, v);
+        case 4 * 16 + 4: return pick_split_depth<4, 4>(n, v);
+        case 4 * 16 + 2: return pick_split_depth<4, 2>(n, v);
+        case 5 * 16 + 5: return pick_split_depth<5, 5>(n, v);
+        case 6 * 16 + 6: return pick_split_depth<6, 6>(n, v);
+        case 6 * 16 + 3: return pick_split_depth<6, 3>(n, v);
+        case 7 * 16 + 7: return pick_split_depth<7, 7>(n, v);
+        case 8 * 16 + 8: return pick_split_depth<8, 8>(n, v);
+        case 8 * 16 + 4: return pick_split_depth<8, 4>(n, v);
+        default: return false;
+    }
+}
+
+// Default float32 family: RPYB_SIG_F32_KERNEL=classic selects the
+// single-pipe compensated kernel, anything else the split kernel.
+int default_f32_family()
+{
+    static int fam = [] {
+        const char* e = getenv("RPYB_SIG_F32_KERNEL");
+        return (e && std::string(e) == "classic") ? kFamilyClassic : kFamilySplit;
+    }();
+    return fam;
+}
+
+// The specialised kernel for (mode, family, width, depth, G); g == 0 takes
+// the default lane shape.  Returns false for shapes served by the generic
+// kernel.
+bool pick_signature_variant(int mode, int family, int d, int n, int g, SigVariant& v)
+{
+    if (n < 2) return false;
+    int gs[4], count = 0;
+    if (!lane_shapes(mode, family, d, gs, &count)) return false;
+    if (g == 0) g = gs[0];
+    if (mode == RPYB_F64) return pick_f64(d, n, g, v);
+    if (family == kFamilyClassic) return pick_classic_f32(d, n, g, v);
+    return pick_split(d, n, g, v);
+}
+
+bool pick_signature_variant(int mode, int d, int n, SigVariant& v)
+{
+    return pick_signature_variant(mode, mode == RPYB_F64 ? kFamilyClassic : default_f32_family(),
+                                  d, n, 0, v);
+}
+
+// Widens float32 increment rows to float64 (the reference run of the
+// error report computes from the same float32 inputs).
+__global__ void widen_rows_kernel(const float* __restrict__ in, double* __restrict__ out, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+// err[s] = max over levels k of ||got_k - ref_k||_inf / ||ref_k||_inf for
+// stream s (the absolute difference where the reference level is zero).
+// One block per stream, levels reduced in shared memory.
+__global__ void level_error_kernel(const float* __restrict__ got, int64_t ld_got,
+                                   const double* __restrict__ ref, int64_t ld_ref, int depth,
+                                   const GenericTables tab, double* __restrict__ err, int64_t n)
+{
+    __shared__ double s_num[32], s_den[32];
+    for (int64_t s = blockIdx.x; s < n; s += gridDim.x) {
+        const float* g = got + s * ld_got;
+        const double* r = ref + s * ld_ref;
+        double worst = 0.0;
+        for (int k = 0; k <= depth; ++k) {
+            double num = 0.0, den = 0.0;
+            for (int64_t i = tab.db[k] + threadIdx.x; i < tab.db[k + 1]; i += blockDim.x) {
+                const double rv = r[i];
+                num = fmax(num, fabs((double)g[i] - rv));
+                den = fmax(den, fabs(rv));
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                num = fmax(num, __shfl_xor_sync(0xffffffffu, num, o));
+                den = fmax(den, __shfl_xor_sync(0xffffffffu, den, o));
+            }
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            __syncthreads();
+            if (lane == 0) {
+                s_num[warp] = num;
+                s_den[warp] = den;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                    num = fmax(num, s_num[w]);
+                    den = fmax(den, s_den[w]);
+                }
+                worst = fmax(worst, den > 0.0 ? num / den : num);
+            }
+        }
+        if (threadIdx.x == 0) err[s] = worst;
+        __syncthreads();
     }
 }
 
@@ -599,6 +1076,161 @@ int signature_fold_interval()
     return fold;
 }
 
+namespace {
+
+// One launch of a specialised signature kernel over n_items work streams
+// (streams, or the time segments of split streams).  `queue` is a zeroed-on-
+// launch device counter of the workspace.  wpb = 0 chooses the block size by
+// occupancy (RPYB_SIG_WPB overrides).  The kernel attribute and the block
+// size are fixed once per device, kernel, per-warp shared memory and forced
+// block size, so repeated launches (and a launch captured into a CUDA graph)
+// only reset the queue and launch.
+int launch_signature_variant(const SigVariant& v, const Geometry& g, int64_t n_items,
+                             const int64_t* offsets, const void* inc, void* out, int64_t ld_out,
+                             const int64_t* order, const int64_t* dst_row, void* alt,
+                             int64_t ld_alt, int* queue, int wpb_forced, cudaStream_t s)
+{
+    SigArgs a{};
+    a.offsets = offsets;
+    a.inc = inc;
+    a.out = out;
+    a.ld_out = ld_out;
+    a.order = order;
+    a.n_streams = n_items;
+    a.items_per_stream = (v.lanes + 31) / 32;
+    a.total_items = a.items_per_stream * n_items;
+    if (a.total_items > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "too many work items");
+    a.queue = queue;
+    a.fold = signature_fold_interval();
+    a.dst_row = dst_row;
+    a.alt = alt;
+    a.ld_alt = ld_alt;
+    for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
+    const size_t smem_warp = v.smem_warp;
+    int wpb = signature_warps_per_block();
+    if (wpb == 0) wpb = (wpb_forced >= 1 && wpb_forced <= kSigWarps) ? wpb_forced : 0;
+    int per_sm = 0;
+    {
+        static std::mutex mu;
+        static std::map<std::tuple<int, const void*, size_t, int>, std::pair<int, int>> chosen;
+        int dev = 0;
+        RPYB_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu);
+        const auto key = std::make_tuple(dev, (const void*)v.fn, smem_warp, wpb);
+        auto it = chosen.find(key);
+        if (it == chosen.end()) {
+            RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(smem_warp * kSigWarps)));
+            int best_wpb = wpb, best_per_sm = 0;
+            if (wpb == 0) {
+                // warps are independent: the block size only matters for
+                // occupancy, so take the one fitting the most warps per SM
+                int best_warps = -1;
+                for (int w = kSigWarps; w >= 1; --w) {
+                    int bps = 0;
+                    RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, v.fn, w * 32,
+                                                                            smem_warp * w));
+                    if (bps * w > best_warps) {
+                        best_warps = bps * w;
+                        best_wpb = w;
+                        best_per_sm = bps;
+                    }
+                }
+            } else {
+                RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&best_per_sm, v.fn,
+                                                                        wpb * 32, smem_warp * wpb));
+            }
+            it = chosen.emplace(key, std::make_pair(best_wpb, best_per_sm)).first;
+        }
+        wpb = it->second.first;
+        per_sm = it->second.second;
+    }
+    if (per_sm < 1) per_sm = 1;
+    const size_t smem = smem_warp * wpb;
+    int64_t blocks = (int64_t)per_sm * device_sm_count();
+    blocks = std::min<int64_t>(blocks, (a.total_items + wpb - 1) / wpb);
+    if (blocks < 1) blocks = 1;
+    RPYB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
+    v.fn<<<(unsigned)blocks, wpb * 32, smem, s>>>(a);
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
+}  // namespace
+
+bool signature_lane_shapes(int mode, int width, int depth, int* gs, int* count)
+{
+    SigVariant v;
+    if (!pick_signature_variant(mode, width, depth, v)) return false;
+    return lane_shapes(mode, mode == RPYB_F64 ? kFamilyClassic : default_f32_family(), width, gs,
+                       count);
+}
+
+int64_t signature_lanes_per_stream(int mode, int width, int depth, int g)
+{
+    SigVariant v;
+    const int family = mode == RPYB_F64 ? kFamilyClassic : default_f32_family();
+    if (!pick_signature_variant(mode, family, width, depth, g, v)) return -1;
+    return v.lanes;
+}
+
+int signature_launch(int mode, int width, int depth, int g_lane, int wpb, int64_t n_items,
+                     const int64_t* offsets, const void* inc, void* out, int64_t ld_out,
+                     const int64_t* order, const int64_t* dst_row, void* alt, int64_t ld_alt,
+                     int* queue, cudaStream_t s)
+{
+    int rc;
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    SigVariant v;
+    const int family = mode == RPYB_F64 ? kFamilyClassic : default_f32_family();
+    if (!pick_signature_variant(mode, family, width, depth, g_lane, v))
+        return fail(RPYB_E_UNSUPPORTED, "no specialised signature kernel for this shape");
+    if (n_items == 0) return RPYB_OK;
+    const bool vec = (mode == RPYB_F32) ? (width % 4 == 0) : (width % 2 == 0);
+    if (vec && (reinterpret_cast<uintptr_t>(inc) & 15) != 0)
+        return fail(RPYB_E_INVALID, "increments must be 16-byte aligned");
+    return launch_signature_variant(v, g, n_items, offsets, inc, out, ld_out, order, dst_row, alt,
+                                    ld_alt, queue, wpb, s);
+}
+
+int signature_error_report(int width, int depth, int64_t n_streams, const int64_t* offsets,
+                           const void* inc32, int64_t total_rows, const void* out32,
+                           int64_t ld_out, const int64_t* order, double* err_out, void* ws,
+                           size_t ws_bytes, cudaStream_t s)
+{
+    int rc;
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
+    const int64_t T = g.size();
+    const int64_t base = up(rpyb_signature_workspace_size(RPYB_F32, width, depth, n_streams));
+    const int64_t refws = up(rpyb_signature_workspace_size(RPYB_F64, width, depth, n_streams));
+    const int64_t refout = up(n_streams * T * 8);
+    const int64_t need = base + refws + refout + up(total_rows * width * 8);
+    if ((int64_t)ws_bytes < need) return fail(RPYB_E_NOMEM, "error-report workspace too small");
+    char* w0 = static_cast<char*>(ws);
+    double* ref = reinterpret_cast<double*>(w0 + base + refws);
+    double* inc64 = reinterpret_cast<double*>(w0 + base + refws + refout);
+    const int64_t nval = total_rows * width;
+    if (nval > 0) {
+        const int64_t blocks = std::min<int64_t>((nval + 255) / 256, 4096);
+        widen_rows_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const float*>(inc32),
+                                                           inc64, nval);
+        RPYB_CUDA(cudaGetLastError());
+    }
+    if ((rc = rpyb_signature(RPYB_F64, width, depth, n_streams, offsets, inc64, ref, T, order,
+                             w0 + base, (size_t)refws, s)))
+        return rc;
+    GenericTables tab{};
+    for (int k = 0; k < kMaxDepth + 2; ++k) tab.db[k] = g.db[k];
+    const int64_t blocks = std::min<int64_t>(n_streams, (int64_t)device_sm_count() * 8);
+    level_error_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, s>>>(
+        static_cast<const float*>(out32), ld_out, ref, T, depth, tab, err_out, n_streams);
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
 }  // namespace rpyb
 
 using namespace rpyb;
@@ -611,8 +1243,7 @@ RPYB_API int64_t rpyb_signature_workspace_size(int mode, int32_t width, int32_t 
     Geometry g;
     if (make_geometry(width, depth, g)) return -1;
     SigVariant v;
-    const bool special = depth >= 2 && ((mode == RPYB_F64) ? pick_variant<true>(width, depth, v)
-                                                           : pick_variant<false>(width, depth, v));
+    const bool special = pick_signature_variant(mode, width, depth, v);
     int64_t bytes = 256;  // queue counter
     if (!special) bytes += n_streams * g.size() * 8;
     return bytes;
@@ -639,82 +1270,17 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
     if ((rc = scratch.get((size_t)need, &ws))) return rc;
 
     SigVariant v{};
-    const bool special = depth >= 2 && ((mode == RPYB_F64) ? pick_variant<true>(width, depth, v)
-                                                           : pick_variant<false>(width, depth, v));
-    const int sms = device_sm_count();
+    const bool special = pick_signature_variant(mode, width, depth, v);
     if (special) {
         if (increments == nullptr) return fail(RPYB_E_INVALID, "null increments");
         const bool vec = (mode == RPYB_F32) ? (width % 4 == 0) : (width % 2 == 0);
         if (vec && (reinterpret_cast<uintptr_t>(increments) & 15) != 0)
             return fail(RPYB_E_INVALID, "increments must be 16-byte aligned");
-        SigArgs a{};
-        a.offsets = offsets;
-        a.inc = increments;
-        a.out = out;
-        a.ld_out = ld_out;
-        a.order = order;
-        a.n_streams = n_streams;
-        a.items_per_stream = (v.lanes + 31) / 32;
-        a.total_items = a.items_per_stream * n_streams;
-        if (a.total_items > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "too many work items");
-        a.queue = static_cast<int*>(ws);
-        a.fold = signature_fold_interval();
-        for (int k = 0; k <= kMaxDepth + 1; ++k) a.db[k] = g.db[k];
-        const size_t esz = (mode == RPYB_F64) ? 8 : 4;
-        const size_t smem_warp = (size_t)v.top_smem_floats * 4 + (size_t)kChunk * width * esz;
-        // Warps are independent, so the block size only matters for occupancy:
-        // take the block size that fits the most warps per SM (registers and
-        // shared memory are both per-warp here), preferring larger blocks.
-        // The attribute and the choice are made once per device, kernel and
-        // per-warp shared memory, so repeated launches (and a launch captured
-        // into a CUDA graph) only reset the queue and launch.
-        int wpb = signature_warps_per_block();
-        int per_sm = 0;
-        {
-            static std::mutex mu;
-            static std::map<std::tuple<int, const void*, size_t>, std::pair<int, int>> chosen;
-            int dev = 0;
-            RPYB_CUDA(cudaGetDevice(&dev));
-            std::lock_guard<std::mutex> lk(mu);
-            const auto key = std::make_tuple(dev, (const void*)v.fn, smem_warp);
-            auto it = chosen.find(key);
-            if (it == chosen.end()) {
-                RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)(smem_warp * kSigWarps)));
-                int best_wpb = wpb, best_per_sm = 0;
-                if (wpb == 0) {
-                    int best_warps = -1;
-                    for (int w = kSigWarps; w >= 1; --w) {
-                        int bps = 0;
-                        RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, v.fn, w * 32,
-                                                                                smem_warp * w));
-                        if (bps * w > best_warps) {
-                            best_warps = bps * w;
-                            best_wpb = w;
-                            best_per_sm = bps;
-                        }
-                    }
-                } else {
-                    RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                        &best_per_sm, v.fn, wpb * 32, smem_warp * wpb));
-                }
-                it = chosen.emplace(key, std::make_pair(best_wpb, best_per_sm)).first;
-            }
-            wpb = it->second.first;
-            per_sm = it->second.second;
-        }
-        if (per_sm < 1) per_sm = 1;
-        const size_t smem = smem_warp * wpb;
-        int64_t blocks = (int64_t)per_sm * sms;
-        const int64_t warps_needed = a.total_items;
-        blocks = std::min<int64_t>(blocks, (warps_needed + wpb - 1) / wpb);
-        if (blocks < 1) blocks = 1;
-        RPYB_CUDA(cudaMemsetAsync(ws, 0, sizeof(int), s));
-        v.fn<<<(unsigned)blocks, wpb * 32, smem, s>>>(a);
-        RPYB_CUDA(cudaGetLastError());
-        return RPYB_OK;
+        return launch_signature_variant(v, g, n_streams, offsets, increments, out, ld_out, order,
+                                        nullptr, nullptr, 0, static_cast<int*>(ws), 0, s);
     }
     // generic path
+    const int sms = device_sm_count();
     double* state = reinterpret_cast<double*>(static_cast<char*>(ws) + 256);
     GenericTables tab;
     for (int k = 0; k < kMaxDepth + 2; ++k) tab.db[k] = g.db[k];
@@ -726,6 +1292,62 @@ RPYB_API int rpyb_signature(int mode, int32_t width, int32_t depth, int64_t n_st
         mode, width, depth, offsets, increments, out, ld_out, n_streams, state, g.size(), tab);
     RPYB_CUDA(cudaGetLastError());
     return RPYB_OK;
+}
+
+RPYB_API int64_t rpyb_signature_batched_workspace_size(int mode, int32_t width, int32_t depth,
+                                                       int64_t n_streams, int64_t total_rows,
+                                                       int with_error)
+{
+    const int64_t base = rpyb_signature_workspace_size(mode, width, depth, n_streams);
+    if (base < 0 || n_streams < 0 || total_rows < 0) return -1;
+    if (!with_error || mode != RPYB_F32) return base;
+    auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
+    const int64_t T = rpyb_tensor_size(width, depth);
+    const int64_t ref = rpyb_signature_workspace_size(RPYB_F64, width, depth, n_streams);
+    return up(base) + up(ref) + up(n_streams * T * 8) + up(total_rows * width * 8);
+}
+
+RPYB_API int rpyb_signature_batched(int mode, int32_t width, int32_t depth, int64_t n_streams,
+                                    const int64_t* offsets, const void* increments,
+                                    int64_t total_rows, void* out, int64_t ld_out,
+                                    const int64_t* order, double* err_out, void* workspace,
+                                    size_t workspace_bytes, void* stream)
+{
+    int rc;
+    if (mode != RPYB_F32 && mode != RPYB_F64)
+        return fail(RPYB_E_INVALID, "unsupported signature mode");
+    Geometry g;
+    if ((rc = make_geometry(width, depth, g))) return rc;
+    if (n_streams < 0 || total_rows < 0) return fail(RPYB_E_INVALID, "negative size");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (err_out == nullptr) {
+        return rpyb_signature(mode, width, depth, n_streams, offsets, increments, out, ld_out,
+                              order, workspace, workspace_bytes, stream);
+    }
+    if (n_streams == 0) return RPYB_OK;
+    if (mode == RPYB_F64) {
+        // the float64 path is its own reference
+        if ((rc = rpyb_signature(mode, width, depth, n_streams, offsets, increments, out, ld_out,
+                                 order, workspace, workspace_bytes, stream)))
+            return rc;
+        RPYB_CUDA(cudaMemsetAsync(err_out, 0, (size_t)n_streams * sizeof(double), s));
+        return RPYB_OK;
+    }
+    if (total_rows > 0 && increments == nullptr) return fail(RPYB_E_INVALID, "null increments");
+    const int64_t need = rpyb_signature_batched_workspace_size(mode, width, depth, n_streams,
+                                                               total_rows, 1);
+    Scratch scratch(workspace, workspace_bytes, s);
+    void* ws = nullptr;
+    if ((rc = scratch.get((size_t)need, &ws))) return rc;
+    // with no rows at all the kernels read no increment; any aligned pointer will do
+    const void* inc32 = (total_rows > 0) ? increments : static_cast<const void*>(ws);
+    const int64_t base = (rpyb_signature_workspace_size(mode, width, depth, n_streams) + 255) /
+                         256 * 256;
+    if ((rc = rpyb_signature(RPYB_F32, width, depth, n_streams, offsets, inc32, out, ld_out,
+                             order, ws, (size_t)base, stream)))
+        return rc;
+    return signature_error_report(width, depth, n_streams, offsets, inc32, total_rows, out,
+                                  ld_out, order, err_out, ws, (size_t)need, s);
 }
 
 }  // extern "C"

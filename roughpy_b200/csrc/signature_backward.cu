@@ -49,6 +49,8 @@
 // mode RPYB_F32 the top-level products (the bulk of the work) and the lanes'
 // per-step gradient partials are float32.
 #include <algorithm>
+#include <climits>
+#include <string>
 
 #include "common.cuh"
 
@@ -138,8 +140,9 @@ signature_backward_kernel(const BwdArgs a)
         const int64_t len = a.offsets[s + 1] - start;
         const int64_t nseg = (len + a.K - 1) / a.K;
         if (nseg > a.max_segments) {
-            // the caller's max_len does not bound this stream: no scratch for
-            // its checkpoints, so its gradient is reported as NaN
+            // unreachable: the host rejects batches whose longest stream
+            // exceeds max_len before launching; kept as a guard so that a
+            // stream without checkpoint scratch never writes past its slot
             for (int64_t e = threadIdx.x; e < len * D; e += blockDim.x)
                 static_cast<T*>(a.grad_inc)[start * D + e] = (T)NAN;
             continue;
@@ -877,6 +880,52 @@ int backward_slots()
     return sms * 2;
 }
 
+// Longest and shortest stream of a batch: out[0] = max length, out[1] =
+// min length (both start at 0 and LLONG_MAX), by atomics over a grid-stride
+// pass through the offsets.
+__global__ void stream_length_range_kernel(const int64_t* __restrict__ offsets, int64_t n,
+                                           long long* out)
+{
+    long long hi = 0, lo = LLONG_MAX;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const long long len = (long long)(offsets[i + 1] - offsets[i]);
+        hi = len > hi ? len : hi;
+        lo = len < lo ? len : lo;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const long long h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+        const long long l2 = __shfl_xor_sync(0xffffffffu, lo, o);
+        hi = h2 > hi ? h2 : hi;
+        lo = l2 < lo ? l2 : lo;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, hi);
+        atomicMin(out + 1, lo);
+    }
+}
+
+// Reads the longest and shortest stream length of the batch into the host
+// values (one small kernel and a 16-byte read that waits for stream s).
+int stream_length_range(const int64_t* offsets, int64_t n, void* scratch16, cudaStream_t s,
+                        int64_t* max_len, int64_t* min_len)
+{
+    long long init[2] = {0, LLONG_MAX};
+    long long got[2] = {0, 0};
+    long long* d = static_cast<long long*>(scratch16);
+    RPYB_CUDA(cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int threads = 256;
+    const int64_t blocks = std::min<int64_t>((n + threads - 1) / threads, 1024);
+    stream_length_range_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, s>>>(offsets,
+                                                                                         n, d);
+    RPYB_CUDA(cudaGetLastError());
+    RPYB_CUDA(cudaMemcpyAsync(got, d, sizeof(got), cudaMemcpyDeviceToHost, s));
+    RPYB_CUDA(cudaStreamSynchronize(s));
+    *max_len = got[0];
+    *min_len = got[1];
+    return RPYB_OK;
+}
+
 }  // namespace
 }  // namespace rpyb
 
@@ -911,12 +960,31 @@ RPYB_API int rpyb_signature_backward(int mode, int32_t width, int32_t depth, int
     if ((rc = make_geometry(width, depth, g))) return rc;
     if (width > 8) return fail(RPYB_E_UNSUPPORTED, "signature backward supports width <= 8");
     if (depth < 1) return fail(RPYB_E_INVALID, "signature backward needs depth >= 1");
-    if (n_streams < 0 || max_len < 0) return fail(RPYB_E_INVALID, "negative size");
+    if (n_streams < 0 || max_len < -1) return fail(RPYB_E_INVALID, "negative size");
     if (checkpoint_every < 1) return fail(RPYB_E_INVALID, "checkpoint interval must be >= 1");
     if (n_streams == 0) return RPYB_OK;
     if (!offsets || !grad_sig || !grad_inc) return fail(RPYB_E_INVALID, "null pointer");
     if (ld_grad != 0 && ld_grad < g.size()) return fail(RPYB_E_INVALID, "ld_grad too small");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // Validate the caller's bound before sizing anything from it: the
+    // checkpoint scratch of every stream is sized by max_len.
+    int64_t longest = 0, shortest = 0;
+    {
+        // 16 bytes of scratch: the head of the caller's workspace when there
+        // is one (rewritten below once the check has completed)
+        Scratch probe(workspace_bytes >= 16 ? workspace : nullptr, workspace_bytes, s);
+        void* p16 = nullptr;
+        if ((rc = probe.get(16, &p16))) return rc;
+        if ((rc = stream_length_range(offsets, n_streams, p16, s, &longest, &shortest))) return rc;
+    }
+    if (shortest < 0) return fail(RPYB_E_INVALID, "offsets must be non-decreasing");
+    if (max_len == -1) {
+        max_len = longest;
+    } else if (longest > max_len) {
+        return fail(RPYB_E_INVALID, "a stream has " + std::to_string(longest) +
+                                        " increments, more than max_len = " +
+                                        std::to_string(max_len));
+    }
     const int64_t need = rpyb_signature_backward_workspace_size(mode, width, depth, n_streams,
                                                                 max_len, checkpoint_every);
     Scratch scratch(workspace, workspace_bytes, s);

@@ -12,6 +12,9 @@ products with compensated accumulation of the running signature).
 """
 from __future__ import annotations
 
+import ctypes
+import json
+
 import numpy as np
 import torch
 
@@ -42,20 +45,25 @@ def longest_first(offsets) -> np.ndarray:
 
 
 class SignaturePlan:
-    """Device-side metadata for one batch layout (offsets + processing order).
+    """One batch layout (offsets + processing order) with its launch schedule.
 
-    Reusable across calls with the same stream lengths; holds the workspace
-    (work-queue counter) so repeated calls allocate nothing.
+    Wraps ``rpyb_sig_plan``: the schedule (lane shape, warps per block and
+    the time-segment length that splits long streams across the GPU) comes
+    from ``RPYB_SIG_SCHEDULE``, the tuning cache, or -- with ``tune`` -- from
+    timing the candidates once for this layout's (width, depth, length, batch)
+    bucket.  Reusable across calls with the same stream lengths; ``run``
+    allocates nothing.  One run at a time per plan.
     """
 
-    def __init__(self, offsets, width: int, depth: int, mode: str = "f32c", device="cuda"):
+    def __init__(self, offsets, width: int, depth: int, mode: str = "f32c", device="cuda",
+                 tune: bool = True):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         self.width = int(width)
         self.depth = int(depth)
         self.mode = mode
         self.code = MODES[mode]
-        off = np.asarray(offsets, dtype=np.int64)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
         if off.ndim != 1 or off.shape[0] < 1 or np.any(np.diff(off) < 0) or off[0] != 0:
             raise ValueError("offsets must be a non-decreasing int array starting at 0")
         self.n_streams = int(off.shape[0] - 1)
@@ -63,39 +71,61 @@ class SignaturePlan:
         self.max_len = int(np.diff(off).max()) if self.n_streams else 0
         self.offsets_host = off
         self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.offsets = torch.from_numpy(off).to(self.device)
         self.order = torch.from_numpy(longest_first(off)).to(self.device)
         self.size = tensor_size(self.width, self.depth)
-        ws = int(_lib.lib.rpyb_signature_workspace_size(self.code, self.width, self.depth,
-                                                        self.n_streams))
-        if ws < 0:
-            raise ValueError(_lib.last_error())
-        self.workspace = torch.empty(max(ws, 1), dtype=torch.uint8, device=self.device)
         self.dtype = torch.float64 if self.code == _lib.F64 else torch.float32
+        self._handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            s = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(_lib.lib.rpyb_sig_plan_create(
+                self.code, self.width, self.depth, self.n_streams, off.ctypes.data,
+                _lib.SIG_PLAN_TUNE if tune else 0, s, ctypes.byref(self._handle)))
 
-    def run(self, increments: torch.Tensor, out: torch.Tensor | None = None,
-            stream: torch.cuda.Stream | None = None) -> torch.Tensor:
-        """Launch on device tensors (no host synchronisation)."""
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            _lib.lib.rpyb_sig_plan_free(h)
+            self._handle = None
+
+    def schedule(self) -> dict:
+        """The plan's launch schedule (lane shape g, warps per block, segment
+        length, work items, merge levels, and where the choice came from)."""
+        buf = ctypes.create_string_buffer(1024)
+        _lib.lib.rpyb_sig_plan_describe(self._handle, buf, len(buf))
+        return json.loads(buf.value.decode())
+
+    def _check_inputs(self, increments):
         if increments.dtype != self.dtype:
             raise TypeError(f"increments must be {self.dtype} for mode {self.mode}")
         if not increments.is_cuda or not increments.is_contiguous():
             raise ValueError("increments must be a contiguous CUDA tensor")
         if increments.numel() != self.total * self.width:
             raise ValueError("increments do not match the offsets")
+
+    def run(self, increments: torch.Tensor, out: torch.Tensor | None = None,
+            stream: torch.cuda.Stream | None = None, report_error: bool = False):
+        """Launch on device tensors (no host synchronisation).
+
+        With ``report_error`` the call returns ``(out, err)``: ``err[s]`` is
+        stream s's largest per-level relative error against the float64 GPU
+        path run on the same increments (zeros in "f64" mode, which is its
+        own reference); the first such call allocates the float64 buffers."""
+        self._check_inputs(increments)
         if out is None:
             out = torch.empty((self.n_streams, self.size), dtype=self.dtype, device=self.device)
-        if self.total == 0:
-            # every stream is empty: the signatures are unit tensors
-            with torch.cuda.stream(stream or torch.cuda.current_stream(self.device)):
-                out.zero_()
-                out[:, 0] = 1.0
-            return out
-        s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
-        _lib.check(_lib.lib.rpyb_signature(
-            self.code, self.width, self.depth, self.n_streams, self.offsets.data_ptr(),
-            increments.data_ptr(), out.data_ptr(), out.stride(0) if out.dim() > 1 else self.size,
-            self.order.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(), s))
-        return out
+        err = None
+        if report_error:
+            err = torch.zeros(self.n_streams, dtype=torch.float64, device=self.device)
+        if self.n_streams:
+            s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+            _lib.check(_lib.lib.rpyb_sig_plan_run(
+                self._handle, increments.data_ptr() if self.total else None, out.data_ptr(),
+                out.stride(0) if out.dim() > 1 else self.size,
+                err.data_ptr() if err is not None else None, s))
+        return (out, err) if report_error else out
 
     def capture(self, increments: torch.Tensor, out: torch.Tensor | None = None):
         """Capture one launch into a CUDA graph: returns ``(graph, out)``.

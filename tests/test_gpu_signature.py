@@ -114,3 +114,42 @@ def test_plan_cuda_graph_replays_with_refilled_inputs(mode):
         want = plan.run(new)
         torch.cuda.synchronize()
         assert torch.equal(gout, want), trial
+
+
+@pytest.mark.parametrize("w,d", [(8, 5), (4, 5), (3, 7)])
+def test_report_error_matches_the_float64_comparison(w, d):
+    """SignaturePlan.run(report_error=True): the per-stream error equals the
+    per-level relative error of the float32 result against the float64 path
+    on the same increments, to 1e-12; rpyb_signature_batched reports the same."""
+    from roughpy_b200 import _lib
+    rng = np.random.default_rng(31 + w)
+    lens = rng.integers(0, 700, size=19)
+    lens[3] = 0
+    off = S.offsets_from_lengths(lens)
+    inc = (rng.normal(size=(int(off[-1]), w)) / 20.0).astype(np.float32)
+    plan = S.SignaturePlan(off, w, d, "f32c")
+    x = torch.from_numpy(inc).cuda()
+    out, err = plan.run(x, report_error=True)
+    plain = plan.run(x)
+    ref = S.SignaturePlan(off, w, d, "f64").run(x.double())
+    torch.cuda.synchronize()
+    assert torch.equal(out, plain)
+    got = err.cpu().numpy()
+    o, r = out.cpu().numpy(), ref.cpu().numpy()
+    want = np.array([level_rel_err(o[s:s + 1], r[s:s + 1], w, d) for s in range(len(lens))])
+    assert np.max(np.abs(got - want)) <= 1e-12
+    assert got[3] == 0.0 and np.max(got) <= 1e-6
+    # the stateless entry point
+    nb = int(_lib.lib.rpyb_signature_batched_workspace_size(_lib.F32, w, d, len(lens),
+                                                             int(off[-1]), 1))
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    out2 = torch.empty_like(out)
+    err2 = torch.empty_like(err)
+    _lib.check(_lib.lib.rpyb_signature_batched(
+        _lib.F32, w, d, len(lens), plan.offsets.data_ptr(), x.data_ptr(), int(off[-1]),
+        out2.data_ptr(), plan.size, plan.order.data_ptr(), err2.data_ptr(), ws.data_ptr(),
+        nb, torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert torch.equal(out2, out) and torch.equal(err2, err)
+    _, e64 = S.SignaturePlan(off, w, d, "f64").run(x.double(), report_error=True)
+    assert float(e64.abs().max()) == 0.0

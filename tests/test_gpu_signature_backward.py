@@ -162,3 +162,41 @@ def test_adjoint_matches_forward_mode_sig_derivative(w, d):
     (S.signature_with_grad(xt, plan) * W).sum().backward()
     rev = (xt.grad * torch.from_numpy(v).cuda()).sum(dim=1)
     assert float((fwd - rev).abs().max()) <= 1e-12 * max(1.0, float(fwd.abs().max()))
+
+
+def _backward_call(plan, x, G, max_len, K=8):
+    from roughpy_b200 import _lib
+    ws_bytes = int(_lib.lib.rpyb_signature_backward_workspace_size(
+        plan.code, plan.width, plan.depth, plan.n_streams, max(plan.max_len, max_len), K))
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device="cuda")
+    gi = torch.full_like(x, 7.0)
+    rc = _lib.lib.rpyb_signature_backward(
+        plan.code, plan.width, plan.depth, plan.n_streams, plan.offsets.data_ptr(), max_len,
+        x.data_ptr(), G.data_ptr(), G.stride(0), gi.data_ptr(), K, ws.data_ptr(), ws.numel(),
+        torch.cuda.current_stream().cuda_stream)
+    return rc, gi
+
+
+def test_backward_rejects_streams_longer_than_max_len_and_accepts_auto():
+    """The C ABI checks the caller's max_len against the offsets before any
+    launch: a bound below the longest stream returns RPYB_E_INVALID and leaves
+    the gradient untouched; max_len = -1 takes the longest stream."""
+    from roughpy_b200 import _lib
+    rng = np.random.default_rng(21)
+    w, d = 3, 4
+    lens = [5, 40, 17]
+    off = S.offsets_from_lengths(lens)
+    plan = S.SignaturePlan(off, w, d, "f64")
+    x = torch.from_numpy(rng.normal(0, 0.3, size=(int(off[-1]), w))).cuda()
+    G = torch.from_numpy(rng.normal(size=(len(lens), plan.size))).cuda()
+    rc, gi = _backward_call(plan, x, G, max_len=39)
+    torch.cuda.synchronize()
+    assert rc == _lib.E_INVALID
+    assert "more than max_len" in _lib.last_error()
+    assert bool((gi == 7.0).all())
+    rc_exact, g_exact = _backward_call(plan, x, G, max_len=40)
+    rc_auto, g_auto = _backward_call(plan, x, G, max_len=-1)
+    torch.cuda.synchronize()
+    assert rc_exact == 0 and rc_auto == 0
+    assert torch.equal(g_exact, g_auto)
+    assert bool(torch.isfinite(g_auto).all())
