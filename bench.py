@@ -173,21 +173,87 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sms)}
 
 
+# ------------------------------------------------------------- ranks
+def rank_workload(rank, world, scaling):
+    """This rank's streams: (lens, off, inc, shard).
+
+    weak: its own 4096-stream batch (seed 2 + rank), shard = (0, 4096);
+    strong: its length-balanced contiguous slice (roughpy_b200.distributed.
+    shard_bounds) of the one 4096-stream batch (seed 2), shard = (lo, hi)."""
+    if scaling == "weak":
+        lens, off, inc = make_workload(seed=2 + rank)
+        return lens, off, inc, (0, N_STREAMS)
+    from roughpy_b200.distributed import shard_bounds
+    lens, off, inc = make_workload(seed=2)
+    lo, hi = shard_bounds(off, world)[rank]
+    local_off = off[lo:hi + 1] - off[lo]
+    return lens[lo:hi], local_off, inc[off[lo]:off[hi]], (int(lo), int(hi))
+
+
+def global_streams(world, scaling):
+    return world * N_STREAMS if scaling == "weak" else N_STREAMS
+
+
+def dry_run(args, rank, world):
+    """The rank plumbing without a GPU: process group (gloo), per-rank
+    workload and shard, barriers, max-over-ranks timing and the JSON line.
+    The timed step is a host copy of the rank's increment rows, so the
+    number measures nothing but the plumbing; the line says so."""
+    import torch
+    import torch.distributed as dist
+    lens, off, inc, shard = rank_workload(rank, world, args.scaling)
+    buf = np.empty_like(inc)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        np.copyto(buf, inc)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        np.copyto(buf, inc)
+    if world > 1:
+        dist.barrier()
+    ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    shards = [None] * world
+    if world > 1:
+        dist.all_gather_object(shards, shard)
+    else:
+        shards = [shard]
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "value": round(global_streams(world, args.scaling) / (ms / 1e3), 1),
+            "unit": "streams/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": args.scaling,
+            "vs_baseline": None, "dtype": "none (dry run)", "data": "synthetic",
+            "dry_run": True,
+            "config": {"workload": "rank plumbing only: the step copies the rank's rows on "
+                                   "the host", "global_batch": global_streams(world, args.scaling),
+                       "shards": shards}}
+
+
 # ------------------------------------------------------------- GPU arm
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from roughpy_b200 import signatures as S
-    from roughpy_b200 import _lib
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    lens, off, inc = make_workload(seed=2 + rank)
+    lens, off, inc, shard = rank_workload(rank, world, args.scaling)
+    n_local = int(len(lens))
     T = S.tensor_size(WIDTH, DEPTH)
     inc_d = torch.from_numpy(inc).to(dev)
     plan = S.SignaturePlan(off, WIDTH, DEPTH, "f32c", device=dev)
-    out_d = torch.empty((N_STREAMS, T), dtype=torch.float32, device=dev)
+    out_d = torch.empty((n_local, T), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    n_global = global_streams(world, args.scaling)
 
     def barrier():
         if world > 1:
@@ -215,13 +281,13 @@ def run_b200(args, rank, world, local_rank):
     barrier()
     ms_total = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = ms_total / args.steps
-    value = world * N_STREAMS / (ms_step / 1e3)
+    value = n_global / (ms_step / 1e3)
 
     # ---- end to end through the C ABI (rpyb_signature_host) from pinned host
     # buffers: host->device copies, kernels and device->host copies, chunked
     # so that the transfers overlap the computation
     inc_h = torch.from_numpy(inc).pin_memory()
-    out_h = torch.empty((N_STREAMS, T), dtype=torch.float32).pin_memory()
+    out_h = torch.empty((n_local, T), dtype=torch.float32).pin_memory()
     for _ in range(args.warmup):
         plan.run_host_pipelined(inc_h, out_h, n_chunks=E2E_CHUNKS)
     barrier()
@@ -234,12 +300,12 @@ def run_b200(args, rank, world, local_rank):
     barrier()
     clk = clocks.stop() if clocks else None
     e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
-    e2e_value = world * N_STREAMS / (e2e_ms / 1e3)
+    e2e_value = n_global / (e2e_ms / 1e3)
 
     # ---- float64 path on the same inputs: speed and the accuracy of float32
     plan64 = S.SignaturePlan(off, WIDTH, DEPTH, "f64", device=dev)
     inc64 = inc_d.double()
-    out64 = torch.empty((N_STREAMS, T), dtype=torch.float64, device=dev)
+    out64 = torch.empty((n_local, T), dtype=torch.float64, device=dev)
     for _ in range(max(1, args.warmup // 2)):
         plan64.run(inc64, out64)
     barrier()
@@ -252,9 +318,11 @@ def run_b200(args, rank, world, local_rank):
     f1.record(stream)
     barrier()
     ms64 = max_over_ranks(f0.elapsed_time(f1)) / k64
-    plan.run(inc_d, out_d)
+    _, err_rows = plan.run(inc_d, out_d, report_error=True)
     torch.cuda.synchronize(dev)
     err = max_over_ranks(level_rel_err_torch(out_d, out64, WIDTH, DEPTH))
+    err_report = max_over_ranks(float(err_rows.max()))
+    del inc64, out64
 
     result = None
     if rank == 0:
@@ -263,8 +331,7 @@ def run_b200(args, rank, world, local_rank):
         fp32_peak = 2 * FP32_LANES_PER_SM * SM_COUNT_B200 * sm_mhz * 1e6 / 1e12
         algo_flops = 2.0 * FMA_PER_STEP * float(lens.sum())
         achieved = algo_flops / (ms_step / 1e3) / 1e12   # this GPU's launch
-        traffic = (SIG_TRAFFIC_BYTES_PER_STREAM * N_STREAMS
-                   if SIG_TRAFFIC_BYTES_PER_STREAM else None)
+        traffic = SIG_TRAFFIC_BYTES_PER_STREAM * n_local if SIG_TRAFFIC_BYTES_PER_STREAM else None
         sweep = fma_sweep(dev, pk["hbm_gbs"]) if not args.no_sweep else None
         result = {
             "metric": METRIC,
@@ -275,22 +342,27 @@ def run_b200(args, rank, world, local_rank):
             "warmup": args.warmup,
             "ms_per_step": round(ms_step, 4),
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": args.scaling,
             "vs_baseline": None,
             "dtype": "f32 (compensated)",
             "data": "synthetic (seeded Brownian increments)",
             "config": {
-                "workload": "uneven batched signatures: 4096 streams/GPU, lengths U{16..4096}, "
-                            "width 8, depth 5, increments N(0,1/len), FP32-comp",
-                "global_batch": world * N_STREAMS,
+                "workload": "uneven batched signatures: 4096 streams "
+                            f"{'per GPU' if args.scaling == 'weak' else 'in all'}, lengths "
+                            "U{16..4096}, width 8, depth 5, increments N(0,1/len), FP32-comp",
+                "global_batch": n_global,
                 "width": WIDTH, "depth": DEPTH,
                 "parallelism": f"dp{world} (streams sharded, no collective)",
+                "shard": list(shard),
+                "schedule": plan.schedule(),
                 "l2": "inputs+outputs 0.9 GB per step > 126 MB L2 (no flush needed)",
             },
-            "f64_path": {"value": round(world * N_STREAMS / (ms64 / 1e3), 1),
-                         "unit": "streams/s", "ms_per_step": round(ms64, 4)},
+            "f64_path": {"value": round(n_global / (ms64 / 1e3), 1),
+                         "unit": "streams/s", "ms_per_step": round(ms64, 4),
+                         "schedule": plan64.schedule()},
             "f32c_speedup_vs_f64": round(ms64 / ms_step, 3),
             "max_rel_err_vs_f64": err,
+            "max_rel_err_reported": err_report,
             "roofline": {
                 "bound": "fp32_fma", "achieved": round(achieved, 3), "peak": round(fp32_peak, 2),
                 "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4),
@@ -298,13 +370,14 @@ def run_b200(args, rank, world, local_rank):
                 "traffic_unit": "bytes per launch (ncu dram read+write, 1024-stream "
                                 "capture scaled by the stream count)",
                 "note": "algorithmic 2*42792 flop per increment; FP32 CUDA-core peak "
-                        "= 148 SM x 128 lanes x 2 x sampled SM clock (no tensor cores on "
-                        "this path)",
+                        "= 148 SM x 128 lanes x 2 x sampled SM clock (computed: no FP32 figure "
+                        "is measured); the float32 kernel also runs its low levels on the "
+                        "FP64 pipe",
             },
             "tensor_mul": sweep,
             "e2e": {"value": round(e2e_value, 1), "unit": "streams/s",
                     "h2d_bytes_per_step": int(inc.nbytes),
-                    "d2h_bytes_per_step": int(N_STREAMS * T * 4),
+                    "d2h_bytes_per_step": int(n_local * T * 4),
                     "ms_per_step": round(e2e_ms, 4),
                     "path": f"rpyb_signature_host, pinned host buffers, {E2E_CHUNKS} chunks "
                             "with copies overlapping kernels"},
@@ -421,6 +494,40 @@ def plain_f64_signatures(dev):
             "cuda_graph": {"value": round(n / (ms_graph / 1e3), 1), "ms": round(ms_graph, 4),
                            "same_output": graph_same},
             "max_rel_err_vs_oracle": err, "cpu_reference_1_core": ref}
+
+
+def long_streams(dev):
+    """A few long streams: 8 streams of 2^17 increments, width 8, depth 5,
+    float32 compensated.  Whole streams leave most of the GPU idle (16 warps
+    each); the tuned plan cuts them into time segments merged by Chen
+    products.  Both schedules are timed on the same inputs."""
+    import torch
+    from roughpy_b200 import signatures as S
+    n, L = 8, 1 << 17
+    rng = np.random.default_rng(6)
+    inc = rng.normal(0, np.sqrt(1.0 / L), size=(n * L, WIDTH)).astype(np.float32)
+    off = np.arange(n + 1, dtype=np.int64) * L
+    x = torch.from_numpy(inc).to(dev)
+    out = torch.empty((n, S.tensor_size(WIDTH, DEPTH)), dtype=torch.float32, device=dev)
+    res = {"workload": "8 streams x 2^17 increments, width 8, depth 5, float32 compensated"}
+    old = os.environ.get("RPYB_SIG_SCHEDULE")
+    try:
+        os.environ["RPYB_SIG_SCHEDULE"] = "seg=0"
+        whole = S.SignaturePlan(off, WIDTH, DEPTH, "f32c", device=dev)
+    finally:
+        if old is None:
+            os.environ.pop("RPYB_SIG_SCHEDULE", None)
+        else:
+            os.environ["RPYB_SIG_SCHEDULE"] = old
+    tuned = S.SignaturePlan(off, WIDTH, DEPTH, "f32c", device=dev, tune=True)
+    for name, plan in (("whole_streams", whole), ("tuned", tuned)):
+        ms = _events_time(torch, lambda: plan.run(x, out), 3, warm=2)
+        res[name] = {"ms": round(ms, 3), "value": round(n / (ms / 1e3), 1), "unit": "streams/s",
+                     "schedule": plan.schedule()}
+    _, err = tuned.run(x, out, report_error=True)
+    res["tuned_max_rel_err_vs_f64"] = float(err.max())
+    res["speedup_tuned_vs_whole"] = round(res["whole_streams"]["ms"] / res["tuned"]["ms"], 2)
+    return res
 
 
 def dyadic_queries(dev):
@@ -542,6 +649,19 @@ def signature_backward(dev):
     for mode, dt in (("f32c", torch.float32), ("f64", torch.float64)):
         launch = _backward_launch(mode, dt, n, L, w, d, inc, W, dev)
         res[mode]["ms_backward_kernel"] = round(_events_time(torch, launch, 3, warm=1), 3)
+    # roofline of the adjoint kernel: a forward recomputation plus the two
+    # adjoint products (with respect to the state and to the increment), each
+    # of the forward's 24,405 FMA per increment at (5,6), all accumulated in
+    # float64 on the FP64 pipe (148 SMs x 64 lanes x 2 flop x clock)
+    fma_per_inc = 24405
+    flops = 2.0 * 3 * fma_per_inc * n * L
+    fp64_peak = 148 * 64 * 2 * 1965e6 / 1e12
+    ms = res["f32c"]["ms_backward_kernel"]
+    ach = flops / (ms / 1e3) / 1e12
+    res["roofline"] = {"bound": "fp64_fma", "achieved": round(ach, 3), "peak": round(fp64_peak, 2),
+                       "unit": "TFLOP/s", "frac": round(ach / fp64_peak, 4),
+                       "note": "algorithmic 3 x 24405 FMA per increment (recomputed forward and "
+                               "the two adjoint products); FP64 peak computed at 1965 MHz"}
     return res
 
 
@@ -693,7 +813,7 @@ def cpu_baseline_leg(workload):
     lens, off, inc = workload
     base = CpuBaseline()
     rng = np.random.default_rng(7)
-    idx = rng.choice(N_STREAMS, size=2 * base.cores, replace=False)
+    idx = rng.choice(len(lens), size=min(2 * base.cores, len(lens)), replace=False)
     n, dt = base.run(sample_streams(inc, off, idx))
     base.close()
     return {"value": round(n / dt, 3), "unit": "streams/s", "cores": base.cores,
@@ -703,16 +823,36 @@ def cpu_baseline_leg(workload):
                       f"float64, one process per core"}
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def relaunch_with_ranks(args) -> int:
+    """`--gpus N` without a launcher: start N ranks on this node with
+    torch.distributed.run (127.0.0.1 rendezvous) and return their status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1",
+           f"--master-port={free_port()}", str(pathlib.Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="weak: 4096 streams per GPU; strong: one 4096-stream batch sharded")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="exercise the rank plumbing on CPU (gloo) without computing")
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
-                    help="skip the plain-f64, dyadic-query and backward workloads")
+                    help="skip the plain-f64, long-stream, dyadic-query and backward workloads")
     ap.add_argument("--profile-backward", type=int, default=0,
                     help="run one adjoint launch on N streams of the backward workload and exit")
     ap.add_argument("--profile-slice", type=int, default=0,
@@ -739,6 +879,8 @@ def main():
         log("note: warmup raised to 3")
         args.warmup = 3
 
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(relaunch_with_ranks(args))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -749,10 +891,22 @@ def main():
             print(json.dumps(res), flush=True)
         return
 
+    import datetime
     import torch
     import torch.distributed as dist
+    if args.dry_run:
+        if world > 1:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        try:
+            res = dry_run(args, rank, world)
+            if res is not None:
+                print(json.dumps(res), flush=True)
+        finally:
+            if world > 1:
+                dist.barrier()
+                dist.destroy_process_group()
+        return
     if world > 1:
-        import datetime
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
@@ -762,6 +916,7 @@ def main():
             if not args.no_extra:
                 dev = torch.device("cuda", local_rank)
                 for key, fn in (("plain_f64_signatures", plain_f64_signatures),
+                                ("long_streams", long_streams),
                                 ("dyadic_queries", dyadic_queries),
                                 ("signature_backward", signature_backward)):
                     try:
