@@ -428,6 +428,26 @@ RPYB_API int rpyb_dyadic_dissect_batch(int64_t n, const double* inf, const doubl
  * interval [block, block+1) * 2^(level - resolution)), or -1.
  */
 typedef struct rpyb_dyadic_tree rpyb_dyadic_tree;
+/*
+ * rpyb_dyadic_save / rpyb_dyadic_load: a built tree as one host byte block
+ * (a fixed header with the tensor shape, mode, resolution and support, the
+ * per-level block tables, then the node table of the mode's type) and back,
+ * so that a stream's cached signatures outlive the process or move to
+ * another device.  save copies the node table to the host and waits for
+ * `stream`; it returns the bytes written (rpyb_dyadic_save_size) or a
+ * negative status.  load validates the block, allocates the nodes on the
+ * current device and copies them there (waiting for `stream`); the loaded
+ * tree answers rpyb_dyadic_query exactly as the saved one.
+ * Replaces: DyadicCachingLayer::dump_cache / load_cache
+ *           (streams/src/dyadic_caching_layer.cpp:168-201), which write the
+ *           resolution-level Lie cache through cereal; here the whole tree
+ *           is saved, so nothing is recomputed after loading.
+ */
+RPYB_API int64_t rpyb_dyadic_save_size(const rpyb_dyadic_tree* tree);
+RPYB_API int64_t rpyb_dyadic_save(const rpyb_dyadic_tree* tree, void* buf, int64_t cap,
+                                  void* stream);
+RPYB_API int rpyb_dyadic_load(const void* buf, int64_t size, rpyb_dyadic_tree** tree,
+                              void* stream);
 #define RPYB_QUERY_RESOLUTION_AUTO (-2147483647 - 1)
 RPYB_API int rpyb_dyadic_build(int mode, int32_t width, int32_t depth, int32_t resolution,
                                double support_inf, double support_sup, int64_t n_events,

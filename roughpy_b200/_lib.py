@@ -93,6 +93,9 @@ SIGNATURES = {
     "rpyb_dyadic_dissect_batch": (_int, [_i64, _vp, _vp, _vp, _int, _vp, _vp, _i64, _vp]),
     "rpyb_dyadic_build": (_int, [_int, _i32, _i32, _i32, _dbl, _dbl, _i64, _vp, _vp, _i32, _vp,
                                  _vp]),
+    "rpyb_dyadic_save_size": (_i64, [_vp]),
+    "rpyb_dyadic_save": (_i64, [_vp, _vp, _i64, _vp]),
+    "rpyb_dyadic_load": (_int, [_vp, _i64, _vp, _vp]),
     "rpyb_dyadic_free": (_int, [_vp]),
     "rpyb_dyadic_tree_info": (_int, [_vp, _vp, _vp, _vp]),
     "rpyb_dyadic_node_row": (_i64, [_vp, _i32, _i64]),

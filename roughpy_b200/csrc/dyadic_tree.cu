@@ -25,7 +25,9 @@
 // (algebra/src/context.cpp:156-215); the signature is exp(l2t(logsig)).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "stream_ops.cuh"
@@ -45,6 +47,20 @@ struct rpyb_dyadic_tree {
 
 namespace rpyb {
 namespace {
+
+// Saved form of a tree (rpyb_dyadic_save / rpyb_dyadic_load): this header,
+// then the per-level tables lo[J+1], cnt[J+1], base[J+1] (int64), then the
+// node table [rows, tensor_size] of the mode's type, all in host byte order.
+constexpr char kTreeMagic[8] = {'R', 'P', 'Y', 'B', 'D', 'Y', 'T', '1'};
+constexpr int64_t kTreeVersion = 1;
+struct SavedTreeHeader {
+    char magic[8];
+    int64_t version;
+    int64_t mode, width, depth, resolution;
+    double support_inf, support_sup;
+    int64_t top_level, unit_row, rows, tensor_size, elem_bytes;
+    int64_t reserved[4];
+};
 
 void release(rpyb_dyadic_tree* t)
 {
@@ -258,6 +274,125 @@ RPYB_API int rpyb_dyadic_build(int mode, int32_t width, int32_t depth, int32_t r
     }
     // ---- levels above the leaves
     if ((rc = build_levels(t, s))) return fail_release(rc);
+    *out_tree = t;
+    return RPYB_OK;
+}
+
+RPYB_API int64_t rpyb_dyadic_save_size(const rpyb_dyadic_tree* t)
+{
+    if (!t) return fail(RPYB_E_INVALID, "null tree");
+    const int64_t es = t->mode == RPYB_F64 ? 8 : 4;
+    return (int64_t)sizeof(SavedTreeHeader) + 3 * (int64_t)(t->J + 1) * 8 +
+           t->rows * t->g.size() * es;
+}
+
+RPYB_API int64_t rpyb_dyadic_save(const rpyb_dyadic_tree* t, void* buf, int64_t cap, void* stream)
+{
+    if (!t) return fail(RPYB_E_INVALID, "null tree");
+    const int64_t need = rpyb_dyadic_save_size(t);
+    if (!buf || cap < need)
+        return fail(RPYB_E_INVALID, "save buffer too small: need " + std::to_string(need) + " bytes");
+    SavedTreeHeader h{};
+    memcpy(h.magic, kTreeMagic, sizeof h.magic);
+    h.version = kTreeVersion;
+    h.mode = t->mode;
+    h.width = t->width;
+    h.depth = t->depth;
+    h.resolution = t->resolution;
+    h.support_inf = t->s0;
+    h.support_sup = t->s1;
+    h.top_level = t->J;
+    h.unit_row = t->unit_row;
+    h.rows = t->rows;
+    h.tensor_size = t->g.size();
+    h.elem_bytes = t->mode == RPYB_F64 ? 8 : 4;
+    char* out = static_cast<char*>(buf);
+    memcpy(out, &h, sizeof h);
+    int64_t* arr = reinterpret_cast<int64_t*>(out + sizeof h);
+    for (int j = 0; j <= t->J; ++j) {
+        arr[j] = t->lo[j];
+        arr[t->J + 1 + j] = t->cnt[j];
+        arr[2 * (t->J + 1) + j] = t->base[j];
+    }
+    char* nodes = out + sizeof h + 3 * (int64_t)(t->J + 1) * 8;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RPYB_CUDA(cudaMemcpyAsync(nodes, t->nodes, (size_t)(t->rows * h.tensor_size * h.elem_bytes),
+                              cudaMemcpyDeviceToHost, s));
+    RPYB_CUDA(cudaStreamSynchronize(s));
+    return need;
+}
+
+RPYB_API int rpyb_dyadic_load(const void* buf, int64_t size, rpyb_dyadic_tree** out_tree,
+                              void* stream)
+{
+    int rc;
+    if (!out_tree) return fail(RPYB_E_INVALID, "null tree handle");
+    *out_tree = nullptr;
+    if (!buf || size < (int64_t)sizeof(SavedTreeHeader))
+        return fail(RPYB_E_INVALID, "not a saved dyadic tree (too short)");
+    SavedTreeHeader h;
+    memcpy(&h, buf, sizeof h);
+    if (memcmp(h.magic, kTreeMagic, sizeof h.magic) != 0)
+        return fail(RPYB_E_INVALID, "not a saved dyadic tree (bad magic)");
+    if (h.version != kTreeVersion) return fail(RPYB_E_INVALID, "unsupported saved-tree version");
+    if (h.mode != RPYB_F32 && h.mode != RPYB_F64) return fail(RPYB_E_INVALID, "bad saved mode");
+    Geometry g;
+    if (h.width < 1 || h.width > (1 << 20) || h.depth < 0 || h.depth > kMaxDepth ||
+        make_geometry((int32_t)h.width, (int32_t)h.depth, g))
+        return fail(RPYB_E_INVALID, "bad saved tensor shape");
+    if (h.tensor_size != g.size() || h.elem_bytes != (h.mode == RPYB_F64 ? 8 : 4) ||
+        h.top_level < 0 || h.top_level > 62 || h.rows < 1 || h.unit_row != h.rows - 1)
+        return fail(RPYB_E_INVALID, "inconsistent saved-tree header");
+    const int64_t J = h.top_level;
+    const int64_t need = (int64_t)sizeof h + 3 * (J + 1) * 8 + h.rows * h.tensor_size * h.elem_bytes;
+    if (size != need) return fail(RPYB_E_INVALID, "saved-tree size does not match its header");
+    const int64_t* arr = reinterpret_cast<const int64_t*>(static_cast<const char*>(buf) + sizeof h);
+    int64_t acc = 0;
+    for (int64_t j = 0; j <= J; ++j) {
+        if (arr[J + 1 + j] < 1 || arr[2 * (J + 1) + j] != acc)
+            return fail(RPYB_E_INVALID, "inconsistent saved-tree level table");
+        acc += arr[J + 1 + j];
+    }
+    if (acc != h.unit_row) return fail(RPYB_E_INVALID, "inconsistent saved-tree level table");
+    const LieMapsDev* maps = nullptr;
+    if ((rc = lie_maps_device(g, &maps))) return rc;
+    rpyb_dyadic_tree* t = new (std::nothrow) rpyb_dyadic_tree();
+    if (!t) return fail(RPYB_E_NOMEM, "out of host memory");
+    if (cudaGetDevice(&t->device) != cudaSuccess) {
+        delete t;
+        return cuda_fail(cudaGetLastError(), "cudaGetDevice");
+    }
+    t->mode = (int)h.mode;
+    t->width = (int32_t)h.width;
+    t->depth = (int32_t)h.depth;
+    t->resolution = (int32_t)h.resolution;
+    t->s0 = h.support_inf;
+    t->s1 = h.support_sup;
+    t->g = g;
+    t->maps = maps;
+    t->J = (int)J;
+    t->unit_row = h.unit_row;
+    t->rows = h.rows;
+    for (int64_t j = 0; j <= J; ++j) {
+        t->lo.push_back(arr[j]);
+        t->cnt.push_back(arr[J + 1 + j]);
+        t->base.push_back(arr[2 * (J + 1) + j]);
+    }
+    const size_t bytes = (size_t)(h.rows * h.tensor_size * h.elem_bytes);
+    if (cudaMalloc(&t->nodes, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        t->nodes = nullptr;
+        release(t);
+        return fail(RPYB_E_NOMEM, "device allocation of the dyadic tree failed");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const char* nodes = static_cast<const char*>(buf) + sizeof h + 3 * (J + 1) * 8;
+    if (cudaMemcpyAsync(t->nodes, nodes, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+        release(t);
+        return rc;
+    }
     *out_tree = t;
     return RPYB_OK;
 }

@@ -37,6 +37,7 @@ from __future__ import annotations
 
 import copy
 import ctypes
+import json
 import math
 
 import numpy as np
@@ -445,6 +446,47 @@ class LieIncrementStream(_StreamQueries):
                 rows_t.data_ptr() if n else None, row_len, ctypes.byref(handle), stream))
         self._tree = _DyadicTree(handle, self.device)
         return self._tree
+
+    # ------------------------------------------------------------- persistence
+    def save(self, path) -> None:
+        """Write the stream (events, shape, resolution, support) and its
+        device dyadic tree (``rpyb_dyadic_save``) to ``path`` (an ``.npz``
+        archive).  The analogue of the reference's cache dump
+        (streams/src/dyadic_caching_layer.cpp:168-201)."""
+        tr = self._build_tree()
+        size = int(_lib.lib.rpyb_dyadic_save_size(tr.handle))
+        if size < 0:
+            _lib.check(size)
+        blob = np.empty(size, dtype=np.uint8)
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            got = int(_lib.lib.rpyb_dyadic_save(tr.handle, blob.ctypes.data, size, stream))
+        if got < 0:
+            _lib.check(got)
+        meta = {"kind": type(self).__name__, "width": self.width, "depth": self.depth,
+                "resolution": self.resolution, "support": [self.support.inf, self.support.sup],
+                "dtype": self.dtype.name, "mode": self.mode}
+        np.savez(path, meta=np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8),
+                 times=self.times, lies=self.lies, tree=blob)
+
+    @classmethod
+    def load(cls, path, device="cuda"):
+        """A stream written by ``save``; its tree is loaded onto ``device``
+        (``rpyb_dyadic_load``) instead of being rebuilt."""
+        with np.load(path) as z:
+            meta = json.loads(bytes(z["meta"]).decode())
+            times, lies, blob = z["times"], z["lies"], np.ascontiguousarray(z["tree"])
+        if meta.get("kind") != cls.__name__:
+            raise TypeError(f"{path} holds a {meta.get('kind')}, not a {cls.__name__}")
+        st = cls(times, lies, meta["width"], meta["depth"], meta["resolution"],
+                 RealInterval(*meta["support"]), np.dtype(meta["dtype"]), meta["mode"], device)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(st.device):
+            stream = torch.cuda.current_stream(st.device).cuda_stream
+            _lib.check(_lib.lib.rpyb_dyadic_load(blob.ctypes.data, blob.size,
+                                                 ctypes.byref(handle), stream))
+        st._tree = _DyadicTree(handle, st.device)
+        return st
 
     # ------------------------------------------------------------- queries
     def _query(self, infs, sups, resolution, logsig=True, sig=False):

@@ -345,3 +345,44 @@ def test_c_abi_query_signatures_are_chen_products_of_events(w, d):
         assert float((lie - ref).abs().max()) <= 1e-11 * scale
     finally:
         _lib.lib.rpyb_dyadic_free(h)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_saved_stream_tree_loads_and_answers_identically(tmp_path, dtype):
+    """LieIncrementStream.save / load (rpyb_dyadic_save / rpyb_dyadic_load):
+    the loaded tree gives bit-identical query results, and damaged blocks are
+    rejected on the host before anything reaches the device."""
+    import ctypes
+    import torch
+    from roughpy_b200 import _lib
+    rng = np.random.default_rng(77)
+    n = 700
+    inc = rng.normal(0, 0.1, size=(n, 4)).astype(dtype)
+    idx = np.sort(rng.uniform(-0.3, 1.2, size=n))
+    st = LieIncrementStream.from_increments(inc, indices=idx, width=4, depth=4, resolution=9)
+    q = np.sort(rng.uniform(-0.5, 1.5, size=(64, 2)), axis=1)
+    want_lie = st.log_signature_batch(q[:, 0], q[:, 1]).cpu()
+    want_sig = st.signature_batch(q[:, 0], q[:, 1]).cpu()
+    path = tmp_path / "stream.npz"
+    st.save(path)
+    back = LieIncrementStream.load(path)
+    assert (back.width, back.depth, back.resolution, back.mode) == (4, 4, 9, st.mode)
+    assert back.support.inf == st.support.inf and back.support.sup == st.support.sup
+    assert back._tree.rows == st._tree.rows and back._tree.top_level == st._tree.top_level
+    assert torch.equal(back.log_signature_batch(q[:, 0], q[:, 1]).cpu(), want_lie)
+    assert torch.equal(back.signature_batch(q[:, 0], q[:, 1]).cpu(), want_sig)
+    # damaged blocks
+    blob = np.ascontiguousarray(np.load(path)["tree"])
+    h = ctypes.c_void_p()
+    s = torch.cuda.current_stream().cuda_stream
+    bad = blob.copy()
+    bad[0] ^= 0xFF
+    assert _lib.lib.rpyb_dyadic_load(bad.ctypes.data, bad.size, ctypes.byref(h), s) == \
+        _lib.E_INVALID
+    short = blob[:-8].copy()
+    assert _lib.lib.rpyb_dyadic_load(short.ctypes.data, short.size, ctypes.byref(h), s) == \
+        _lib.E_INVALID
+    assert not h.value
+    from roughpy_b200.streams import TickStream
+    with pytest.raises(TypeError):
+        TickStream.load(path)
