@@ -64,6 +64,12 @@ RPYB_API const char* rpyb_version(void);
  * memory of every device to the driver.  No reference counterpart.
  */
 RPYB_API int rpyb_release_cached_memory(void);
+/*
+ * Bytes of the current device's scratch pool in use by calls in flight and
+ * held in reserve (0 and 0 before the first pooled call).  No reference
+ * counterpart.
+ */
+RPYB_API int rpyb_scratch_pool_usage(int64_t* used_bytes, int64_t* reserved_bytes);
 
 /* Number of scalars in a width/depth tensor: (width^(depth+1)-1)/(width-1). */
 RPYB_API int64_t rpyb_tensor_size(int32_t width, int32_t depth);
@@ -143,9 +149,11 @@ RPYB_API int rpyb_ft_exp(int dtype, int32_t width, int32_t depth, int64_t batch,
  * rpyb_ft_exp_noalloc_max_bytes() bytes (8 MiB) that every GPU loading the
  * library holds until exit.  Calls needing more (batch * tensor_size *
  * element size) fail with RPYB_E_INVALID.  The first call on a device looks
- * up the array's device address; make it before any stream capture.  All
- * calls on a device share the array, so calls that overlap on the GPU race:
- * order them on one stream or with events.
+ * up the array's device address; make it before any stream capture.  The
+ * address is kept for the life of the process: do not reset the device
+ * (cudaDeviceReset) between calls, which would reload the module elsewhere.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * race: order them on one stream or with events.
  */
 RPYB_API int64_t rpyb_ft_exp_noalloc_max_bytes(void);
 RPYB_API int rpyb_ft_exp_noalloc(int dtype, int32_t width, int32_t depth, int64_t batch,

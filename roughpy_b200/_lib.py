@@ -45,6 +45,7 @@ SIGNATURES = {
     "rpyb_last_error": (ctypes.c_char_p, []),
     "rpyb_version": (ctypes.c_char_p, []),
     "rpyb_release_cached_memory": (_int, []),
+    "rpyb_scratch_pool_usage": (_int, [_vp, _vp]),
     "rpyb_tensor_size": (_i64, [_i32, _i32]),
     "rpyb_ft_fma": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _pi32, _vp]),
     "rpyb_ft_mul_gather": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,

@@ -72,12 +72,18 @@ RPYB_API int rpyb_ft_exp_noalloc(int dtype, int32_t width, int32_t depth, int64_
                                  void* out, const void* arg, int64_t ld_out, int64_t ld_arg,
                                  int32_t out_depth, void* stream)
 {
-    const int64_t need = rpyb_ft_exp_workspace_size(dtype, width, depth, batch);
-    if (need < 0) return fail(RPYB_E_INVALID, "invalid dtype, width or depth");
-    if ((size_t)need > kNoAllocScratchBytes)
+    if (batch < 0) return fail(RPYB_E_INVALID, "rpyb_ft_exp_noalloc: negative batch");
+    // bound the batch by division first: the byte count of a huge batch
+    // would overflow int64 and could pass a product-based check
+    const int64_t per_row = rpyb_ft_exp_workspace_size(dtype, width, depth, 1);
+    if (per_row <= 0) return fail(RPYB_E_INVALID, "invalid dtype, width or depth");
+    if (batch > (int64_t)kNoAllocScratchBytes / per_row)
         return fail(RPYB_E_INVALID,
-                    "rpyb_ft_exp_noalloc: batch * tensor_size * element_size = " +
-                        std::to_string(need) + " bytes exceeds the 8 MiB static scratch");
+                    "rpyb_ft_exp_noalloc: batch " + std::to_string(batch) + " needs more than the " +
+                        "8 MiB static scratch (" + std::to_string(per_row) + " bytes per row)");
+    const int64_t need = rpyb_ft_exp_workspace_size(dtype, width, depth, batch);
+    if (need < 0 || (size_t)need > kNoAllocScratchBytes)
+        return fail(RPYB_E_INVALID, "rpyb_ft_exp_noalloc: scratch size out of range");
     if (batch <= 0) return rpyb_ft_exp(dtype, width, depth, batch, out, arg, ld_out, ld_arg,
                                        out_depth, nullptr, 0, stream);
     void* scratch = nullptr;

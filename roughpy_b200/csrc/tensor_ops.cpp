@@ -161,6 +161,23 @@ RPYB_API int rpyb_release_cached_memory(void)
     return RPYB_OK;
 }
 
+RPYB_API int rpyb_scratch_pool_usage(int64_t* used_bytes, int64_t* reserved_bytes)
+{
+    int dev = 0;
+    RPYB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(RPYB_E_UNSUPPORTED, "device ordinal too large");
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    uint64_t used = 0, reserved = 0;
+    if (g_pools[dev]) {
+        RPYB_CUDA(cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrUsedMemCurrent, &used));
+        RPYB_CUDA(cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrReservedMemCurrent,
+                                          &reserved));
+    }
+    if (used_bytes) *used_bytes = (int64_t)used;
+    if (reserved_bytes) *reserved_bytes = (int64_t)reserved;
+    return RPYB_OK;
+}
+
 RPYB_API const char* rpyb_last_error(void) { return rpyb::g_last_error.c_str(); }
 
 RPYB_API const char* rpyb_version(void) { return "roughpy_b200 0.1.0 (sm_100a)"; }

@@ -290,13 +290,27 @@ class _StreamQueries:
         (default: the stream's) (streams/src/stream.cpp:232-258).  As in the
         reference the new stream keeps the underlying stream's own support
         (not one set by ``restrict``) and takes ``resolution`` as its
-        default; ``depth`` (or ``ctx.depth``) truncates the pieces."""
+        default; ``ctx.depth`` (a context wins over ``depth``, and its width
+        must be the stream's) or ``depth`` truncates the pieces.  A depth
+        above the stream's is rejected: the device tree holds the stream's
+        depth only, where the reference would build a deeper context."""
         if not isinstance(partition, Partition):
             partition = Partition(*partition)
-        if ctx is not None and depth is None:
+        # the binding parses resolution and depth as C ints ("i"): a float is
+        # a TypeError there, and a context takes precedence over depth
+        for name, v in (("resolution", resolution), ("depth", depth)):
+            if v is not None and not isinstance(v, (int, np.integer)):
+                raise TypeError(f"{name} must be an integer, not {type(v).__name__}")
+        if ctx is not None:
+            if int(getattr(ctx, "width", self.width)) != self.width:
+                raise ValueError("context width must match stream width")
             depth = getattr(ctx, "depth", None)
         res = self.resolution if resolution is None else int(resolution)
-        d = self.depth if not depth else min(int(depth), self.depth)
+        if depth and int(depth) > self.depth:
+            # the reference would build a deeper context (get_alike); the
+            # device tree holds the stream's depth only
+            raise ValueError(f"depth {int(depth)} exceeds the stream's depth {self.depth}")
+        d = self.depth if not depth else int(depth)
         ivs = [partition[i] for i in range(len(partition))]
         infs = np.array([iv.inf for iv in ivs])
         sups = np.array([iv.sup for iv in ivs])

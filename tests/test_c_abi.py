@@ -107,3 +107,17 @@ def test_python_errors_match_reference_types():
         _internals._basis_wd(None)
     with pytest.raises(TypeError):
         _internals._dtype_code(np.int32)
+
+
+def test_noalloc_size_checks_cannot_overflow():
+    """rpyb_ft_exp_noalloc bounds the batch by division, so a batch whose
+    byte count would overflow int64 is rejected like any oversized one, and
+    a negative batch has its own message; both before any device work."""
+    from roughpy_b200 import _lib
+    big = 1 << 62
+    assert _lib.lib.rpyb_ft_exp_noalloc(_lib.F64, 8, 5, big, 16, 16, 37449, 37449, -1,
+                                        None) == _lib.E_INVALID
+    assert "static scratch" in _lib.last_error()
+    assert _lib.lib.rpyb_ft_exp_noalloc(_lib.F32, 8, 5, -1, 16, 16, 37449, 37449, -1,
+                                        None) == _lib.E_INVALID
+    assert "negative batch" in _lib.last_error()

@@ -370,3 +370,26 @@ def test_restated_stream_of_lie_elements(golden):
     lie = st.log_signature(0.0, 1.0)
     np.testing.assert_array_equal(lie[:3], seq[0])
     assert not np.any(lie[3:])
+
+
+def test_simplify_argument_rules_follow_the_binding():
+    """roughpy/src/streams/stream.cpp:410-468: resolution and depth are C ints
+    (a float is a TypeError), a context takes precedence over depth and must
+    have the stream's width.  A depth above the stream's is rejected (the
+    device tree holds the stream's depth).  All checks run on the host before
+    any device work."""
+    import types
+    from roughpy_b200.streams import LieIncrementStream, Partition, RealInterval
+    st = LieIncrementStream.from_increments(np.zeros((4, 3)), width=3, depth=3)
+    part = Partition(RealInterval(0.0, 1.0), [0.5])
+    with pytest.raises(TypeError):
+        st.simplify(part, resolution=2.0)
+    with pytest.raises(TypeError):
+        st.simplify(part, depth=2.5)
+    with pytest.raises(ValueError, match="width"):
+        st.simplify(part, ctx=types.SimpleNamespace(width=2, depth=2))
+    with pytest.raises(ValueError, match="exceeds"):
+        st.simplify(part, depth=4)
+    # the context wins over depth: a valid depth does not rescue a bad context
+    with pytest.raises(ValueError, match="exceeds"):
+        st.simplify(part, ctx=types.SimpleNamespace(width=3, depth=5), depth=2)

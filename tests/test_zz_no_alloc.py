@@ -64,3 +64,35 @@ def test_noalloc_rejects_sizes_beyond_the_static_scratch():
     rc = _lib.lib.rpyb_ft_exp_noalloc(_lib.F64, w, d, batch, 16, 16, T, T, -1, None)
     assert rc == _lib.E_INVALID
     assert "static scratch" in _lib.last_error()
+
+
+def _pool_usage():
+    import ctypes
+    used, reserved = ctypes.c_int64(), ctypes.c_int64()
+    _lib.check(_lib.lib.rpyb_scratch_pool_usage(ctypes.byref(used), ctypes.byref(reserved)))
+    return used.value, reserved.value
+
+
+def test_noalloc_takes_nothing_from_the_library_pool():
+    """The contract itself: two calls leave the library's scratch pool empty
+    (no pooled allocation in use or reserved), while the regular entry point
+    given no workspace does draw on it, which shows that the probe sees a
+    pooled allocation when one happens."""
+    w, d, batch = 4, 5, 64
+    T = int(_lib.lib.rpyb_tensor_size(w, d))
+    rng = np.random.default_rng(5)
+    x = torch.from_numpy(rng.normal(0, 0.5, size=(batch, T))).to("cuda", torch.float64)
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib.rpyb_release_cached_memory())
+    before = _pool_usage()
+    assert before == (0, 0)
+    for _ in range(2):
+        _exp_noalloc(_lib.F64, w, d, x)
+    torch.cuda.synchronize()
+    assert _pool_usage() == before
+    out = torch.zeros_like(x)
+    _lib.check(_lib.lib.rpyb_ft_exp(_lib.F64, w, d, batch, out.data_ptr(), x.data_ptr(), T, T, -1,
+                                    None, 0, torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert _pool_usage()[1] >= batch * T * 8
+    _lib.check(_lib.lib.rpyb_release_cached_memory())
