@@ -129,6 +129,30 @@ class LieBasis:
     def size(self) -> int:
         return int(self.degree_begin[self.depth + 1]) - 1
 
+    # Value semantics as in the reference type (roughpy/compute/_src/
+    # lie_basis.c:520-610): bases are equal when width, depth, degree_begin
+    # and the Hall data agree, and the hash covers the same fields.
+    def _key(self):
+        n = self.size() + 1
+        return (self.width, self.depth, self.degree_begin[:self.depth + 2].tobytes(),
+                self.data[:n].tobytes())
+
+    def __hash__(self):
+        h = self.__dict__.get("_hash")
+        if h is None:
+            h = hash(("LieBasis",) + self._key())
+            self._hash = h
+        return h
+
+    def __eq__(self, other):
+        if not isinstance(other, LieBasis):
+            return NotImplemented
+        return self._key() == other._key()
+
+    def __ne__(self, other):
+        eq = self.__eq__(other)
+        return eq if eq is NotImplemented else not eq
+
     def _csr(self, which: int, dtype) -> SparseMatrix:
         key = (which, np.dtype(dtype).str)
         if key not in self._maps:

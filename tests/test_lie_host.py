@@ -54,3 +54,17 @@ def test_t2l_inverts_l2t_on_lie_elements():
     x = rng.standard_normal((4, lb.size()))
     back = csr_apply(lb.get_t2l_matrix(), csr_apply(lb.get_l2t_matrix(), x))
     np.testing.assert_array_almost_equal(back, x, decimal=15)
+
+
+def test_lie_basis_value_semantics():
+    """As the reference's LieBasis type (tests/compute/test_lie_basis.py:24-140):
+    equal shape means equal bases and equal hashes, usable as set members and
+    dict keys; a different width or depth differs."""
+    from roughpy_b200 import compute as rpc
+    a, b = rpc.LieBasis(3, 4), rpc.LieBasis(3, 4)
+    c, d = rpc.LieBasis(4, 4), rpc.LieBasis(3, 5)
+    assert a == b and hash(a) == hash(b) and not (a != b)
+    assert a != c and a != d and c != d
+    assert len({a, b, c}) == 2
+    assert len({hash(rpc.LieBasis(2, 3)), hash(rpc.LieBasis(3, 2)), hash(rpc.LieBasis(4, 5))}) == 3
+    assert (a == 3) is False
