@@ -593,82 +593,33 @@ signature_kernel_split(const SigArgs a)
             __syncwarp();
             if (t0 + kChunk + lane < len) load_row<float, D>(nx, xs + (t0 + kChunk + lane) * D);
 
-#pragma unroll 1
-            for (int j = 0; j < nsteps; ++j) {
-                const float* row = x32 + j * D;
-                const double* row64 = x64 + j * D;
-                float x[D];
-                load_row_smem<float, D>(x, row);
-                float xa[G];
-                if constexpr (SUBS == 1) {
-#pragma unroll
-                    for (int g = 0; g < G; ++g) xa[g] = x[g];
-                } else {
-                    load_slice<float, G>(xa, row + sub * G);
-                }
+            // Software pipeline: the float64 part of step j+1 (its two Horner
+            // chains and the path update, which need only the path words after
+            // step j) is issued before the float32 products of step j, so the
+            // latency of the float64 chain and its conversion hides behind the
+            // FFMA2s instead of stalling the warp every step.
+            float x[D], accx, accm;
+            // chains and path update of step jj: reads the path words before
+            // the step, leaves them after it
+            auto chains = [&](int jj, float& ax, float& am) {
+                const double* row64 = x64 + jj * D;
                 double xc[PP];
 #pragma unroll
                 for (int i = 0; i < P; ++i) xc[i] = row64[c[i]];
-
-                // ---- top level: chain through the path (f64), residual and
-                // products (f32)
-                float accx = 0.5f;
+                ax = 0.5f;
+                am = 1.f;
                 if constexpr (P > 0) {
                     double acc = fma(xc[0], 1.0 / N, ph[0]);
 #pragma unroll
                     for (int i = 2; i <= P; ++i) acc = fma(acc, xc[i - 1] * (1.0 / (N - i + 1)), ph[i - 1]);
-                    accx = (float)(acc * 0.5);
+                    ax = (float)(acc * 0.5);
+                    double accm64 = fma(xc[0], 1.0 / (N - 1), ph[0]);
+#pragma unroll
+                    for (int i = 2; i <= P; ++i)
+                        accm64 = fma(accm64, xc[i - 1] * (1.0 / (N - i)), ph[i - 1]);
+                    am = (float)accm64;
                 }
-                float r[G];
-                if constexpr (PACK_M) {
-#pragma unroll
-                    for (int g = 0; g < G; g += 2) {
-                        const float2 q = __ffma2_rn(make_float2(accx, accx), make_float2(xa[g], xa[g + 1]),
-                                                    make_float2(md[g], md[g + 1]));
-                        r[g] = q.x;
-                        r[g + 1] = q.y;
-                    }
-                } else {
-#pragma unroll
-                    for (int g = 0; g < G; ++g) r[g] = fmaf(accx, xa[g], md[g]);
-                }
-#pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    if constexpr (PACK_T) {
-                        const float2 r2 = make_float2(r[g], r[g]);
-#pragma unroll
-                        for (int h = 0; h < D / 2; ++h) {
-                            const float2 q = __ffma2_rn(r2, make_float2(x[2 * h], x[2 * h + 1]),
-                                                        make_float2(td[g][2 * h], td[g][2 * h + 1]));
-                            td[g][2 * h] = q.x;
-                            td[g][2 * h + 1] = q.y;
-                        }
-                    } else {
-#pragma unroll
-                        for (int b = 0; b < D; ++b) td[g][b] = fmaf(r[g], x[b], td[g][b]);
-                    }
-                }
-                // ---- level N-1: chain (f64), deltas (f32)
-                float accm = 1.f;
-                if constexpr (P > 0) {
-                    double acc = fma(xc[0], 1.0 / (N - 1), ph[0]);
-#pragma unroll
-                    for (int i = 2; i <= P; ++i) acc = fma(acc, xc[i - 1] * (1.0 / (N - i)), ph[i - 1]);
-                    accm = (float)acc;
-                }
-                if constexpr (PACK_M) {
-#pragma unroll
-                    for (int g = 0; g < G; g += 2) {
-                        const float2 q = __ffma2_rn(make_float2(accm, accm), make_float2(xa[g], xa[g + 1]),
-                                                    make_float2(md[g], md[g + 1]));
-                        md[g] = q.x;
-                        md[g + 1] = q.y;
-                    }
-                } else {
-#pragma unroll
-                    for (int g = 0; g < G; ++g) md[g] = fmaf(accm, xa[g], md[g]);
-                }
-                // ---- path levels k = P .. 1 (f64)
+                // path levels k = P .. 1 (top-down: each reads pre-step words)
 #pragma unroll
                 for (int k = P; k >= 1; --k) {
                     if (k == 1) {
@@ -680,7 +631,79 @@ signature_kernel_split(const SigArgs a)
                         ph[k - 1] = fma(acc, xc[k - 1], ph[k - 1]);
                     }
                 }
+            };
+            // float32 products of a step: top words, then the mid deltas
+            auto products = [&](const float (&xv)[D], float ax, float am) {
+                float xa[G];
+                if constexpr (SUBS == 1) {
+#pragma unroll
+                    for (int g = 0; g < G; ++g) xa[g] = xv[g];
+                } else {
+                    // the lane's G letters of level N-1 (SUBS > 1: a slice of the
+                    // row, chosen by selects so that xv stays in registers)
+#pragma unroll
+                    for (int g = 0; g < G; ++g) xa[g] = xv[g];
+#pragma unroll
+                    for (int q = 1; q < SUBS; ++q)
+#pragma unroll
+                        for (int g = 0; g < G; ++g) xa[g] = (sub == q) ? xv[q * G + g] : xa[g];
+                }
+                float r[G];
+                if constexpr (PACK_M) {
+#pragma unroll
+                    for (int g = 0; g < G; g += 2) {
+                        const float2 q = __ffma2_rn(make_float2(ax, ax), make_float2(xa[g], xa[g + 1]),
+                                                    make_float2(md[g], md[g + 1]));
+                        r[g] = q.x;
+                        r[g + 1] = q.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int g = 0; g < G; ++g) r[g] = fmaf(ax, xa[g], md[g]);
+                }
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    if constexpr (PACK_T) {
+                        const float2 r2 = make_float2(r[g], r[g]);
+#pragma unroll
+                        for (int h = 0; h < D / 2; ++h) {
+                            const float2 q = __ffma2_rn(r2, make_float2(xv[2 * h], xv[2 * h + 1]),
+                                                        make_float2(td[g][2 * h], td[g][2 * h + 1]));
+                            td[g][2 * h] = q.x;
+                            td[g][2 * h + 1] = q.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < D; ++b) td[g][b] = fmaf(r[g], xv[b], td[g][b]);
+                    }
+                }
+                if constexpr (PACK_M) {
+#pragma unroll
+                    for (int g = 0; g < G; g += 2) {
+                        const float2 q = __ffma2_rn(make_float2(am, am), make_float2(xa[g], xa[g + 1]),
+                                                    make_float2(md[g], md[g + 1]));
+                        md[g] = q.x;
+                        md[g + 1] = q.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int g = 0; g < G; ++g) md[g] = fmaf(am, xa[g], md[g]);
+                }
+            };
+            load_row_smem<float, D>(x, x32);
+            chains(0, accx, accm);
+#pragma unroll 1
+            for (int j = 0; j + 1 < nsteps; ++j) {
+                float xn[D], axn, amn;
+                load_row_smem<float, D>(xn, x32 + (j + 1) * D);
+                chains(j + 1, axn, amn);
+                products(x, accx, accm);
+#pragma unroll
+                for (int i = 0; i < D; ++i) x[i] = xn[i];
+                accx = axn;
+                accm = amn;
             }
+            products(x, accx, accm);
 
             // ---- fold the chunk: top += m64 * X + td, mid += md (float64)
             if (lane < D) {

@@ -385,8 +385,11 @@ __device__ __forceinline__ void lower_unit(const ChainArgs& a, int64_t li, int& 
 }
 
 // NT > 0: the depth is NT (the top level's split loop is unrolled)
+#ifndef RPYB_CHAIN_MIN_BLOCKS
+#define RPYB_CHAIN_MIN_BLOCKS 1
+#endif
 template <typename TS, int D, int V, int TU, int NT>
-__global__ void __launch_bounds__(kChainThreads, 1)
+__global__ void __launch_bounds__(kChainThreads, RPYB_CHAIN_MIN_BLOCKS)
 chain_products_kernel(const ChainArgs a)
 {
     constexpr int NB = D / V;
