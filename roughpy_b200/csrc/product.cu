@@ -491,6 +491,18 @@ int tile_words()
     return w;
 }
 
+// RPYB_F32_WIDE=1: float32 rows at widths 6 and 8 own twice the last
+// letters per thread (V = 6 and 4), so each thread keeps twice the bytes in
+// flight (a float32 word is half a float64 one)
+bool f32_wide_blocks()
+{
+    static const bool on = [] {
+        const char* e = getenv("RPYB_F32_WIDE");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 // Width -> last-letter block V of the one-letter blocked kernel (0: none);
 // float64 rows at width 4 use a block of 2 (more resident warps)
 int blocked_v_one(int width, bool f64 = false)
@@ -499,8 +511,8 @@ int blocked_v_one(int width, bool f64 = false)
         case 3: return 3;
         case 4: return f64 ? 2 : 4;
         case 5: return 5;
-        case 6: return 3;
-        case 8: return 2;
+        case 6: return (!f64 && f32_wide_blocks()) ? 6 : 3;
+        case 8: return (!f64 && f32_wide_blocks()) ? 4 : 2;
         default: return 0;
     }
 }
@@ -562,8 +574,18 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
                 product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
             break;
         case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
-        case 6: product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
-        case 8: product_kernel_blocked<T, TR, 8, 2, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6:
+            if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks())
+                product_kernel_blocked<T, TR, 6, 6, ACC, 2><<<grid, kThreads, 0, stream>>>(a);
+            else
+                product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+            break;
+        case 8:
+            if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks())
+                product_kernel_blocked<T, TR, 8, 4, ACC, 2><<<grid, kThreads, 0, stream>>>(a);
+            else
+                product_kernel_blocked<T, TR, 8, 2, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+            break;
         default: return fail(RPYB_E_UNSUPPORTED, "no blocked product kernel for this width");
     }
     RPYB_CUDA(cudaGetLastError());
