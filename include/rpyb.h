@@ -495,6 +495,22 @@ RPYB_API int rpyb_piecewise_query(int32_t width, int32_t depth, int64_t n_pieces
                                   void* stream);
 
 /*
+ * Batched Campbell-Baker-Hausdorff products: for each list q, with items
+ * i in [offsets_host[q], offsets_host[q+1]) of `lies` (device float64
+ * [items, ld_lies] Hall coordinates),
+ *   out[q] = t2l(log(exp(l2t(x_first)) ... exp(l2t(x_last))))
+ * in float64 (device [n_lists, ld_out]).  A one-element list returns its
+ * element, an empty list zero, as the reference does.  Temporaries are
+ * stream-ordered allocations; the call waits for `stream` when a list has a
+ * single element (the host index table of that copy must outlive it).
+ * Replaces: Context::cbh (algebra/src/context.cpp:187-208), one list per call
+ *           in the reference.
+ */
+RPYB_API int rpyb_cbh(int32_t width, int32_t depth, int64_t n_lists, const int64_t* offsets_host,
+                      const double* lies, int64_t ld_lies, double* out, int64_t ld_out,
+                      void* stream);
+
+/*
  * Forward-mode derivative of signatures along Lie perturbations, batched over
  * independent lists.  List q holds the pairs i in [offsets_host[q],
  * offsets_host[q+1]) of rows of `logsig` (the log-signature of an interval)

@@ -103,6 +103,7 @@ SIGNATURES = {
     "rpyb_dyadic_query": (_int, [_vp, _i64, _vp, _vp, _i32, _vp, _i64, _vp, _i64, _vp]),
     "rpyb_piecewise_query": (_int, [_i32, _i32, _i64, _vp, _vp, _vp, _i64, _dbl, _dbl, _i32,
                                     _i64, _vp, _vp, _i32, _vp, _i64, _vp, _i64, _vp]),
+    "rpyb_cbh": (_int, [_i32, _i32, _i64, _vp, _vp, _i64, _vp, _i64, _vp]),
     "rpyb_sig_derivative_workspace_size": (_i64, [_int, _i32, _i32, _i64, _i64]),
     "rpyb_sig_derivative": (_int, [_int, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
                                    _sz, _vp]),

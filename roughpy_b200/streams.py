@@ -714,6 +714,42 @@ def sig_derivative(pairs, width: int, depth: int, device="cuda") -> np.ndarray:
     return out[0].cpu().numpy()
 
 
+def cbh_batch(lies, offsets, width: int, depth: int, device="cuda") -> torch.Tensor:
+    """Campbell-Baker-Hausdorff products of many lists of Lie elements
+    (``rpyb_cbh``): list q holds rows ``offsets[q]:offsets[q+1]`` of ``lies``
+    (Hall coordinates, [items, c] with c <= the Lie dimension).  Returns a
+    float64 device tensor [n_lists, lie_dim]; row q is Context::cbh of the
+    list (algebra/src/context.cpp:187-208)."""
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    L = rpc.LieBasis(width, depth).size()
+    rows = np.asarray(lies, dtype=np.float64).reshape(-1, np.shape(lies)[-1] if np.ndim(lies) > 1
+                                                       else L)
+    full = np.zeros((rows.shape[0], L))
+    full[:, :min(L, rows.shape[1])] = rows[:, :L]
+    n = off.shape[0] - 1
+    dev = torch.device(device)
+    out = torch.zeros((n, L), dtype=torch.float64, device=dev)
+    if n == 0:
+        return out
+    x = torch.from_numpy(full).to(dev)
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib.rpyb_cbh(int(width), int(depth), n, off.ctypes.data,
+                                     x.data_ptr() if rows.shape[0] else None, L, out.data_ptr(),
+                                     L, stream))
+    return out
+
+
+def cbh(lies, width: int, depth: int, device="cuda") -> np.ndarray:
+    """Context::cbh of one sequence of Lie elements (Hall coordinates)."""
+    rows = [np.asarray(x, dtype=np.float64).reshape(-1) for x in lies]
+    L = rpc.LieBasis(width, depth).size()
+    mat = np.zeros((len(rows), L))
+    for i, r in enumerate(rows):
+        mat[i, :min(L, r.size)] = r[:L]
+    return cbh_batch(mat, [0, len(rows)], width, depth, device)[0].cpu().numpy()
+
+
 class _DyadicTree:
     """Owner of an rpyb_dyadic_tree handle (device memory freed with it)."""
 

@@ -386,3 +386,25 @@ def test_saved_stream_tree_loads_and_answers_identically(tmp_path, dtype):
     from roughpy_b200.streams import TickStream
     with pytest.raises(TypeError):
         TickStream.load(path)
+
+
+@pytest.mark.parametrize("w,d", [(2, 4), (3, 3), (4, 3)])
+def test_batched_cbh_against_the_restated_context(golden, w, d):
+    """rpyb_cbh (roughpy_b200.streams.cbh_batch) against the restated
+    Context::cbh (algebra/src/context.cpp:187-208) on lists of 0, 1, 2 and 7
+    Lie elements, including a zero element; a single element comes back
+    unchanged."""
+    from roughpy_b200.streams import cbh, cbh_batch
+    a = _arith(golden, w, d)
+    rng = np.random.default_rng(w * 10 + d)
+    sizes = [2, 0, 1, 7, 3]
+    lists = [[rng.normal(0, 0.3, size=a.L) for _ in range(k)] for k in sizes]
+    lists[3][2] = np.zeros(a.L)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    flat = np.array([x for lst in lists for x in lst])
+    got = cbh_batch(flat, off, w, d).cpu().numpy()
+    for q, lst in enumerate(lists):
+        want = a.cbh(lst) if lst else np.zeros(a.L)
+        lie_close(got[q], want, 1e-12)
+    assert np.array_equal(got[2], lists[2][0])
+    lie_close(cbh(lists[0], w, d), a.cbh(lists[0]), 1e-12)
