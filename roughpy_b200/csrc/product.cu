@@ -491,14 +491,15 @@ int tile_words()
     return w;
 }
 
-// RPYB_F32_WIDE=1: float32 rows at widths 6 and 8 own twice the last
-// letters per thread (V = 6 and 4), so each thread keeps twice the bytes in
-// flight (a float32 word is half a float64 one)
+// float32 rows at width 8 own four last letters per thread (twice the
+// float64 block), so each thread keeps as many bytes in flight as a float64
+// one (measured on B200: (8,6) 1.36 -> 1.27 ms; a block of six at width 6
+// was slower, so width 6 keeps three).  RPYB_F32_WIDE=0 restores two.
 bool f32_wide_blocks()
 {
     static const bool on = [] {
         const char* e = getenv("RPYB_F32_WIDE");
-        return e && e[0] == '1';
+        return !(e && e[0] == '0');
     }();
     return on;
 }
@@ -511,7 +512,7 @@ int blocked_v_one(int width, bool f64 = false)
         case 3: return 3;
         case 4: return f64 ? 2 : 4;
         case 5: return 5;
-        case 6: return (!f64 && f32_wide_blocks()) ? 6 : 3;
+        case 6: return 3;
         case 8: return (!f64 && f32_wide_blocks()) ? 4 : 2;
         default: return 0;
     }
@@ -574,12 +575,7 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
                 product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
             break;
         case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
-        case 6:
-            if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks())
-                product_kernel_blocked<T, TR, 6, 6, ACC, 2><<<grid, kThreads, 0, stream>>>(a);
-            else
-                product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
-            break;
+        case 6: product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
         case 8:
             if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks())
                 product_kernel_blocked<T, TR, 8, 4, ACC, 2><<<grid, kThreads, 0, stream>>>(a);

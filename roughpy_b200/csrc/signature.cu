@@ -1144,6 +1144,10 @@ int launch_signature_variant(const SigVariant& v, const Geometry& g, int64_t n_i
         if (it == chosen.end()) {
             RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)(smem_warp * kSigWarps)));
+            // the whole unified L1/shared array as shared memory: the kernels
+            // stage their state there and read global memory once per chunk
+            RPYB_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared));
             int best_wpb = wpb, best_per_sm = 0;
             if (wpb == 0) {
                 // warps are independent: the block size only matters for
