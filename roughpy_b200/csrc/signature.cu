@@ -53,6 +53,11 @@ constexpr int kChunk = 32;    // increment rows staged per warp in shared memory
 #ifndef RPYB_SIG_SPLIT_MAXREG
 #define RPYB_SIG_SPLIT_MAXREG 192
 #endif
+// with the top level in TMEM shared memory no longer limits the warps per
+// SM; 168 registers fit three blocks of four warps
+#ifndef RPYB_SIG_TMEM_MAXREG
+#define RPYB_SIG_TMEM_MAXREG 168
+#endif
 
 // level-(N-1) words per lane of the float64 kernel at width 8
 #ifndef RPYB_SIG_F64_G8
@@ -482,6 +487,47 @@ signature_kernel(const SigArgs a)
 }
 
 // ------------------------------------------------------------------------
+// Tensor memory (TMEM) as per-warp storage.  Each SM has 128 lanes x 512
+// columns of 32-bit TMEM next to its tensor cores; warp w of a block reads
+// and writes lanes 32 (w % 4) .. 32 (w % 4) + 31 with tcgen05.ld / st, one
+// lane per thread.  The split kernel below keeps its float64 top-level
+// values there instead of in shared memory when `TM` is set (no MMA is
+// issued; TMEM only holds state).
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr));
+}
+__device__ __forceinline__ void tmem_st16(uint32_t addr, const uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+        :
+        : "r"(addr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]),
+          "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]),
+          "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// TMEM columns a block of nwarps warps takes: 128 per warp in each lane
+// quarter (64 float64 values per thread), a power of two
+__host__ __device__ constexpr int tmem_cols_for(int nwarps) { return nwarps <= 4 ? 128 : 256; }
+
+// ------------------------------------------------------------------------
 // float32 mode on both arithmetic pipes ("split" kernel).
 //
 // The classic float32 kernel above spends a third of its FP32 pipe on work
@@ -506,8 +552,8 @@ signature_kernel(const SigArgs a)
 // (FFMA2), while m64 * X[b] is added in float64 when the chunk's deltas are
 // folded (one DFMA per word per chunk).  Per step and lane the FP32 pipe sees
 // G*D + 2G FMAs, every one of them a useful Horner FMA.
-template <int D, int N, int G>
-__global__ void __maxnreg__(RPYB_SIG_SPLIT_MAXREG)
+template <int D, int N, int G, bool TM>
+__global__ void __maxnreg__(TM ? RPYB_SIG_TMEM_MAXREG : RPYB_SIG_SPLIT_MAXREG)
 signature_kernel_split(const SigArgs a)
 {
     constexpr int P = N - 2;                 // path levels 1..N-2
@@ -519,21 +565,40 @@ signature_kernel_split(const SigArgs a)
     constexpr bool PACK_T = (D % 2 == 0);    // top words in f32x2 pairs
     constexpr bool PACK_M = (G % 2 == 0);    // mid words in f32x2 pairs
 
-    // dynamic shared memory per warp: top values [TOPW][32] f64, mid values
-    // [G][32] f64, chunk sums [D] f64 (16-byte padded), staged rows
-    // [kChunk][D] f64 then [kChunk][D] f32
+    // dynamic shared memory per warp: top values [TOPW][32] f64 (unless they
+    // live in TMEM), mid values [G][32] f64, chunk sums [D] f64 (16-byte
+    // padded), staged rows [kChunk][D] f64 then [kChunk][D] f32
+    static_assert(!TM || TOPW == 64, "TMEM top level: 64 words per lane (width 8, G = 8)");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    constexpr int TOPS = TM ? 0 : TOPW;     // top words kept in shared memory
     constexpr size_t kXsumBytes = ((size_t)D * 8 + 15) / 16 * 16;
-    constexpr size_t kWarpBytes = (size_t)(TOPW + G) * 32 * 8 + kXsumBytes +
+    constexpr size_t kWarpBytes = (size_t)(TOPS + G) * 32 * 8 + kXsumBytes +
                                   (size_t)kChunk * D * 12;
     unsigned char* wbase = smem_raw + (size_t)warp * kWarpBytes;
     double* top64 = reinterpret_cast<double*>(wbase);
-    double* mid64 = top64 + TOPW * 32;
+    double* mid64 = top64 + TOPS * 32;
     double* xsum = mid64 + G * 32;
-    double* x64 = reinterpret_cast<double*>(wbase + (size_t)(TOPW + G) * 32 * 8 + kXsumBytes);
+    double* x64 = reinterpret_cast<double*>(wbase + (size_t)(TOPS + G) * 32 * 8 + kXsumBytes);
     float* x32 = reinterpret_cast<float*>(x64 + kChunk * D);
+
+    // TMEM for the top level: allocated by warp 0 for the whole block, freed
+    // by it after every warp has left the work loop
+    __shared__ uint32_t s_tmem_base;
+    uint32_t ttop = 0;   // this warp's TMEM address (lane quarter, first column)
+    const int nwarps_blk = (int)(blockDim.x >> 5);
+    if constexpr (TM) {
+        if (warp == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                         :: "r"(smem_u32(&s_tmem_base)), "r"(tmem_cols_for(nwarps_blk)));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
+        tmem_fence_before();
+        __syncthreads();
+        tmem_fence_after();
+        ttop = s_tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * (warp >> 2));
+    }
 
     while (true) {
         int item = 0;
@@ -575,7 +640,15 @@ signature_kernel_split(const SigArgs a)
             for (int b = 0; b < D; ++b) td[g][b] = 0.f;
         }
 #pragma unroll 4
-        for (int w = 0; w < TOPW + G; ++w) top64[w * 32 + lane] = 0.0;
+        for (int w = 0; w < TOPS + G; ++w) top64[w * 32 + lane] = 0.0;
+        if constexpr (TM) {
+            uint32_t z[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) z[i] = 0u;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) tmem_st16(ttop + 16 * q, z);
+            tmem_wait_st();
+        }
 
         float nx[D];
         if (lane < len) load_row<float, D>(nx, xs + (int64_t)lane * D);
@@ -718,18 +791,48 @@ signature_kernel_split(const SigArgs a)
             for (int g = 0; g < G; ++g) {
                 double* mp = mid64 + g * 32 + lane;
                 const double m = *mp;
+                if constexpr (TM) {
+                    // the 8 top words of mid word g: 16 TMEM columns (lo, hi)
+                    uint32_t r[16];
+                    tmem_ld16(ttop + 16 * g, r);
+                    tmem_wait_ld();
 #pragma unroll
-                for (int b = 0; b < D; ++b) {
-                    double* tp = top64 + (g * D + b) * 32 + lane;
-                    *tp = fma(m, X[b], *tp + (double)td[g][b]);
-                    td[g][b] = 0.f;
+                    for (int b = 0; b < D; ++b) {
+                        double t = __hiloint2double((int)r[2 * b + 1], (int)r[2 * b]);
+                        t = fma(m, X[b], t + (double)td[g][b]);
+                        r[2 * b] = (uint32_t)__double2loint(t);
+                        r[2 * b + 1] = (uint32_t)__double2hiint(t);
+                        td[g][b] = 0.f;
+                    }
+                    tmem_st16(ttop + 16 * g, r);
+                } else {
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        double* tp = top64 + (g * D + b) * 32 + lane;
+                        *tp = fma(m, X[b], *tp + (double)td[g][b]);
+                        td[g][b] = 0.f;
+                    }
                 }
                 *mp = m + (double)md[g];
                 md[g] = 0.f;
             }
+            if constexpr (TM) tmem_wait_st();
         }
 
         // ---- write the stream's words owned by this lane
+        float ttv[TM ? TOPW : 1];
+        if constexpr (TM) {
+            // warp-wide TMEM reads (every lane takes part, active or not)
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                uint32_t r[16];
+                tmem_ld16(ttop + 16 * g, r);
+                tmem_wait_ld();
+#pragma unroll
+                for (int b = 0; b < D; ++b)
+                    ttv[g * D + b] = (float)__hiloint2double((int)r[2 * b + 1], (int)r[2 * b]);
+            }
+        }
         if (active) {
             float* __restrict__ o = output_row<float>(a, s);
             if (beta == 0) o[0] = 1.f;
@@ -749,7 +852,10 @@ signature_kernel_split(const SigArgs a)
                 o[a.db[N - 1] + mw] = (float)mid64[g * 32 + lane];
                 float tv[D];
 #pragma unroll
-                for (int b = 0; b < D; ++b) tv[b] = (float)top64[(g * D + b) * 32 + lane];
+                for (int b = 0; b < D; ++b) {
+                    if constexpr (TM) tv[b] = ttv[g * D + b];
+                    else tv[b] = (float)top64[(g * D + b) * 32 + lane];
+                }
                 if constexpr (D % 4 == 0) {
                     // a lane's D top words below one mid word are contiguous
                     float* dst = o + a.db[N] + mw * D;
@@ -762,6 +868,14 @@ signature_kernel_split(const SigArgs a)
                 for (int b = 0; b < D; ++b) o[a.db[N] + mw * D + b] = tv[b];
             }
         }
+    }
+    if constexpr (TM) {
+        tmem_fence_before();
+        __syncthreads();
+        tmem_fence_after();
+        if (warp == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                         :: "r"(s_tmem_base), "r"(tmem_cols_for(nwarps_blk)));
     }
 }
 
@@ -825,6 +939,7 @@ struct SigVariant {
     int g;
     int64_t lanes;          // W: lanes per stream
     size_t smem_warp;       // dynamic shared memory per warp (bytes)
+    bool tmem = false;      // top level in TMEM: blocks of at most 4 warps, 4 blocks per SM
 };
 
 template <bool F64, int D, int N, int G, bool HS>
@@ -836,13 +951,24 @@ SigVariant make_variant()
     return SigVariant{&signature_kernel<F64, D, N, G, HS>, G, W, top + stage};
 }
 
-template <int D, int N, int G>
+template <int D, int N, int G, bool TM = false>
 SigVariant make_split_variant()
 {
     constexpr int64_t W = IPow<D, N - 2>::value * (D / G);
     constexpr size_t xsum = ((size_t)D * 8 + 15) / 16 * 16;
-    constexpr size_t bytes = (size_t)(G * D + G) * 32 * 8 + xsum + (size_t)kChunk * D * 12;
-    return SigVariant{&signature_kernel_split<D, N, G>, G, W, bytes};
+    constexpr size_t bytes = (size_t)((TM ? 0 : G * D) + G) * 32 * 8 + xsum + (size_t)kChunk * D * 12;
+    return SigVariant{&signature_kernel_split<D, N, G, TM>, G, W, bytes, TM};
+}
+
+// The split kernel's top level in TMEM at width 8 (RPYB_SIG_TMEM=0: in
+// shared memory)
+bool split_tmem_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("RPYB_SIG_TMEM");
+        return !(e && e[0] == '0');
+    }();
+    return on;
 }
 
 template <bool F64, int D, int G, bool HS>
@@ -867,6 +993,18 @@ bool pick_depth(int n, SigVariant& v)
 template <int D, int G>
 bool pick_split_depth(int n, SigVariant& v)
 {
+    if constexpr (D == 8 && G == 8) {
+        if (split_tmem_enabled()) {
+            switch (n) {
+                case 2: v = make_split_variant<D, 2, G, true>(); return true;
+                case 3: v = make_split_variant<D, 3, G, true>(); return true;
+                case 4: v = make_split_variant<D, 4, G, true>(); return true;
+                case 5: v = make_split_variant<D, 5, G, true>(); return true;
+                case 6: v = make_split_variant<D, 6, G, true>(); return true;
+                default: return false;
+            }
+        }
+    }
     switch (n) {
         case 2: v = make_split_variant<D, 2, G>(); return true;
         case 3: v = make_split_variant<D, 3, G>(); return true;
@@ -1152,11 +1290,14 @@ int launch_signature_variant(const SigVariant& v, const Geometry& g, int64_t n_i
             if (wpb == 0) {
                 // warps are independent: the block size only matters for
                 // occupancy, so take the one fitting the most warps per SM
+                // (TMEM variants: blocks of up to 4 warps, 4 blocks per SM,
+                // so that the blocks' TMEM never exceeds the SM's 512 columns)
                 int best_warps = -1;
-                for (int w = kSigWarps; w >= 1; --w) {
+                for (int w = v.tmem ? 4 : kSigWarps; w >= 1; --w) {
                     int bps = 0;
                     RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, v.fn, w * 32,
                                                                             smem_warp * w));
+                    if (v.tmem) bps = std::min(bps, 512 / tmem_cols_for(w));
                     if (bps * w > best_warps) {
                         best_warps = bps * w;
                         best_wpb = w;
@@ -1166,6 +1307,7 @@ int launch_signature_variant(const SigVariant& v, const Geometry& g, int64_t n_i
             } else {
                 RPYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&best_per_sm, v.fn,
                                                                         wpb * 32, smem_warp * wpb));
+                if (v.tmem) best_per_sm = std::min(best_per_sm, 512 / tmem_cols_for(wpb));
             }
             it = chosen.emplace(key, std::make_pair(best_wpb, best_per_sm)).first;
         }
