@@ -1314,6 +1314,16 @@ int launch_signature_variant(const SigVariant& v, const Geometry& g, int64_t n_i
         wpb = it->second.first;
         per_sm = it->second.second;
     }
+    {
+        // RPYB_SIG_BLOCKS_PER_SM forces the resident blocks per SM the grid
+        // is sized for (the occupancy calculator's figure otherwise)
+        static const int forced_bps = [] {
+            const char* e = getenv("RPYB_SIG_BLOCKS_PER_SM");
+            const int b = e ? atoi(e) : 0;
+            return (b >= 1 && b <= 32) ? b : 0;
+        }();
+        if (forced_bps) per_sm = v.tmem ? std::min(forced_bps, 512 / tmem_cols_for(wpb)) : forced_bps;
+    }
     if (per_sm < 1) per_sm = 1;
     const size_t smem = smem_warp * wpb;
     int64_t blocks = (int64_t)per_sm * device_sm_count();
