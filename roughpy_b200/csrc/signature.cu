@@ -74,7 +74,8 @@ struct SigArgs {
     int64_t items_per_stream;
     int64_t total_items;
     int* queue;   // device work counter (zeroed before launch)
-    int fold;     // fold interval of the compensated mode (steps)
+    int fold;     // fold interval of the classic compensated mode (steps)
+    int fold_chunks;  // split kernel: chunks of kChunk steps between folds
     // output rows: row s of `out` unless dst_row is given, in which case
     // r = dst_row[s] selects row r of `out` (r >= 0) or row ~r of `alt`
     // (r < 0; the segment rows of split streams)
@@ -641,6 +642,8 @@ signature_kernel_split(const SigArgs a)
         }
 #pragma unroll 4
         for (int w = 0; w < TOPS + G; ++w) top64[w * 32 + lane] = 0.0;
+        if (lane < D) xsum[lane] = 0.0;
+        int chunks_since_fold = 0;
         if constexpr (TM) {
             uint32_t z[16];
 #pragma unroll
@@ -763,27 +766,40 @@ signature_kernel_split(const SigArgs a)
                     for (int g = 0; g < G; ++g) md[g] = fmaf(am, xa[g], md[g]);
                 }
             };
+            // two steps per iteration with alternating register sets, so
+            // that the pipeline needs no register copies
+            float x1[D], ax1, am1;
             load_row_smem<float, D>(x, x32);
             chains(0, accx, accm);
+            int j = 0;
 #pragma unroll 1
-            for (int j = 0; j + 1 < nsteps; ++j) {
-                float xn[D], axn, amn;
-                load_row_smem<float, D>(xn, x32 + (j + 1) * D);
-                chains(j + 1, axn, amn);
+            for (; j + 2 < nsteps; j += 2) {
+                load_row_smem<float, D>(x1, x32 + (j + 1) * D);
+                chains(j + 1, ax1, am1);
                 products(x, accx, accm);
-#pragma unroll
-                for (int i = 0; i < D; ++i) x[i] = xn[i];
-                accx = axn;
-                accm = amn;
+                load_row_smem<float, D>(x, x32 + (j + 2) * D);
+                chains(j + 2, accx, accm);
+                products(x1, ax1, am1);
             }
-            products(x, accx, accm);
+            if (j + 1 < nsteps) {
+                load_row_smem<float, D>(x1, x32 + (j + 1) * D);
+                chains(j + 1, ax1, am1);
+                products(x, accx, accm);
+                products(x1, ax1, am1);
+            } else {
+                products(x, accx, accm);
+            }
 
-            // ---- fold the chunk: top += m64 * X + td, mid += md (float64)
+            // the chunk's increment sum joins the fold period's sum X
             if (lane < D) {
-                double sum = 0.0;
-                for (int j = 0; j < nsteps; ++j) sum += x64[j * D + lane];
+                double sum = xsum[lane];
+                for (int jj = 0; jj < nsteps; ++jj) sum += x64[jj * D + lane];
                 xsum[lane] = sum;
             }
+            // ---- fold every fold_chunks chunks and at the stream's end:
+            // top += m64 * X + td, mid += md (float64)
+            if (++chunks_since_fold < a.fold_chunks && t0 + kChunk < len) continue;
+            chunks_since_fold = 0;
             __syncwarp();
             double X[D];
             load_row_smem<double, D>(X, xsum);
@@ -817,6 +833,8 @@ signature_kernel_split(const SigArgs a)
                 md[g] = 0.f;
             }
             if constexpr (TM) tmem_wait_st();
+            __syncwarp();
+            if (lane < D) xsum[lane] = 0.0;
         }
 
         // ---- write the stream's words owned by this lane
@@ -1239,6 +1257,17 @@ int signature_fold_interval()
     return fold;
 }
 
+// Chunks of 32 steps between the split kernel's folds (RPYB_SIG_SPLIT_FOLD)
+int split_fold_chunks()
+{
+    static int f = [] {
+        const char* e = getenv("RPYB_SIG_SPLIT_FOLD");
+        const int v = e ? atoi(e) : 2;
+        return (v >= 1 && v <= 64) ? v : 2;
+    }();
+    return f;
+}
+
 namespace {
 
 // One launch of a specialised signature kernel over n_items work streams
@@ -1265,6 +1294,7 @@ int launch_signature_variant(const SigVariant& v, const Geometry& g, int64_t n_i
     if (a.total_items > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "too many work items");
     a.queue = queue;
     a.fold = signature_fold_interval();
+    a.fold_chunks = split_fold_chunks();
     a.dst_row = dst_row;
     a.alt = alt;
     a.ld_alt = ld_alt;
