@@ -46,10 +46,10 @@ E2E_CHUNKS = 16
 SM_COUNT_B200 = 148
 FP32_LANES_PER_SM = 128
 # DRAM bytes (read + write) per stream of the float32 signature kernel on this
-# workload: 68.1 + 97.4 MB measured by ncu on the 1024-stream slice
+# workload: 68.1 + 98.2 MB measured by ncu on the 1024-stream slice
 # (`bench.py --profile-slice 1024`, profiles/signature_w8d5_f32c_f64.md); the
 # traffic is inputs plus outputs, so it scales with the number of streams.
-SIG_TRAFFIC_BYTES_PER_STREAM = (68.1e6 + 97.4e6) / 1024
+SIG_TRAFFIC_BYTES_PER_STREAM = (68.1e6 + 98.2e6) / 1024
 
 
 def log(*a):
