@@ -462,6 +462,19 @@ RPYB_API int rpyb_dyadic_build(int mode, int32_t width, int32_t depth, int32_t r
                                const double* times_host, const void* rows, int32_t row_len,
                                rpyb_dyadic_tree** tree, void* stream);
 RPYB_API int rpyb_dyadic_free(rpyb_dyadic_tree* tree);
+/*
+ * Range-product table of a tree: with blocks of 2^block_log2 leaves (0 picks
+ * about the square root of the leaf count), the product of the leaves from
+ * each leaf to its block's ends (both ways) and a disjoint sparse table over
+ * the blocks, computed in float64 and stored in the tree's type.  A later
+ * rpyb_dyadic_query whose pieces are no finer than the leaves and span more
+ * than one block then multiplies at most four table rows instead of every
+ * piece (the same product, associated differently).  The table doubles the
+ * tree's device memory; trees of fewer than four blocks get none.  Waits for
+ * `stream`.  No reference counterpart: the reference recomputes coarse
+ * pieces recursively (streams/src/dyadic_caching_layer.cpp:86-154).
+ */
+RPYB_API int rpyb_dyadic_range_table(rpyb_dyadic_tree* tree, int32_t block_log2, void* stream);
 RPYB_API int rpyb_dyadic_tree_info(const rpyb_dyadic_tree* tree, int64_t* rows,
                                    int32_t* top_level, const void** nodes);
 RPYB_API int64_t rpyb_dyadic_node_row(const rpyb_dyadic_tree* tree, int32_t level,

@@ -98,6 +98,7 @@ SIGNATURES = {
     "rpyb_dyadic_save": (_i64, [_vp, _vp, _i64, _vp]),
     "rpyb_dyadic_load": (_int, [_vp, _i64, _vp, _vp]),
     "rpyb_dyadic_free": (_int, [_vp]),
+    "rpyb_dyadic_range_table": (_int, [_vp, _i32, _vp]),
     "rpyb_dyadic_tree_info": (_int, [_vp, _vp, _vp, _vp]),
     "rpyb_dyadic_node_row": (_i64, [_vp, _i32, _i64]),
     "rpyb_dyadic_query": (_int, [_vp, _i64, _vp, _vp, _i32, _vp, _i64, _vp, _i64, _vp]),

@@ -41,8 +41,17 @@ struct rpyb_dyadic_tree {
     int J = 0;                              // top level
     std::vector<int64_t> lo, cnt, base;     // per level: first block, blocks, first row
     int64_t unit_row = 0, rows = 0;
-    void* nodes = nullptr;                  // [rows, T] of the mode's type
+    void* nodes = nullptr;                  // [rows (+ table rows), T] of the mode's type
     const rpyb::LieMapsDev* maps = nullptr;
+    // range-product table (rpyb_dyadic_range_table), rows after the tree's:
+    // blocks of 2^tb leaves (tree level tb); pre[i] / suf[i] = product of the
+    // leaves from leaf i's block start to i / from i to its block end;
+    // dst[l][c] = the disjoint sparse table over the blocks (level l >= 1:
+    // the product from block c to the middle of its 2^l group, or from the
+    // middle to c)
+    int tb = -1;
+    int64_t pre_base = 0, suf_base = 0, dst_base = 0;
+    int dst_levels = 0;
 };
 
 namespace rpyb {
@@ -81,6 +90,34 @@ int64_t node_row(const rpyb_dyadic_tree* t, int64_t level, int64_t blk)
     const int64_t rel = blk - t->lo[level];
     if (rel < 0 || rel >= t->cnt[level]) return -1;
     return t->base[level] + rel;
+}
+
+// Tree rows covering the leaf range [a, e) in order (greedy maximal aligned
+// blocks; blocks the tree does not hold, outside the leaf range, are units
+// and skipped).
+void range_nodes(const rpyb_dyadic_tree* t, int64_t a, int64_t e, std::vector<int64_t>& out)
+{
+    while (a < e) {
+        int j = 0;
+        while (j < t->J && (a >> (j + 1)) * ((int64_t)2 << j) == a && a + ((int64_t)2 << j) <= e &&
+               node_row(t, j + 1, a >> (j + 1)) >= 0)
+            ++j;
+        const int64_t row = node_row(t, j, a >> j);
+        if (row >= 0) out.push_back(row);
+        a += (int64_t)1 << j;
+    }
+}
+
+// float64 accumulator rows acc[i] -> tree-typed rows dst[i] (mode's type)
+template <typename T>
+__global__ void store_rows_kernel(T* __restrict__ nodes, int64_t T_, const double* __restrict__ acc,
+                                  const int64_t* __restrict__ dst, int64_t n)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * T_;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / T_, c = e - r * T_;
+        nodes[dst[r] * T_ + c] = (T)acc[e];
+    }
 }
 
 int build_levels(rpyb_dyadic_tree* t, cudaStream_t s)
@@ -278,6 +315,126 @@ RPYB_API int rpyb_dyadic_build(int mode, int32_t width, int32_t depth, int32_t r
     return RPYB_OK;
 }
 
+RPYB_API int rpyb_dyadic_range_table(rpyb_dyadic_tree* t, int32_t block_log2, void* stream)
+{
+    int rc;
+    if (!t) return fail(RPYB_E_INVALID, "null tree");
+    if (block_log2 < 0 || block_log2 > 30) return fail(RPYB_E_INVALID, "block_log2 out of range");
+    const int64_t n0 = t->cnt[0];
+    int b = block_log2;
+    if (b == 0) {
+        // blocks of about sqrt(leaves), at least 16 leaves
+        b = 4;
+        while (b < 30 && ((int64_t)1 << (2 * (b + 1))) <= n0) ++b;
+    }
+    if (t->tb >= 0) return RPYB_OK;                       // already built
+    if (b > t->J || n0 < ((int64_t)4 << b)) return RPYB_OK;  // too small to pay off
+    const Geometry& g = t->g;
+    const int64_t T = g.size();
+    const int64_t es = t->mode == RPYB_F64 ? 8 : 4;
+    const int64_t nb = t->cnt[b], lob = t->lo[b], lo0 = t->lo[0];
+    int levels = 0;
+    while (((int64_t)1 << levels) < nb) ++levels;
+    // factor lists (tree rows) of every table entry, in table-row order
+    std::vector<int64_t> off{0}, rows_list;
+    off.reserve(2 * n0 + (size_t)levels * nb + 1);
+    for (int side = 0; side < 2; ++side) {
+        for (int64_t i = 0; i < n0; ++i) {
+            const int64_t k = lo0 + i;
+            const int64_t bs = std::max((k >> b) * ((int64_t)1 << b), lo0);
+            const int64_t be = std::min(((k >> b) + 1) * ((int64_t)1 << b), lo0 + n0);
+            if (side == 0) range_nodes(t, bs, k + 1, rows_list);   // pre
+            else range_nodes(t, k, be, rows_list);                 // suf
+            off.push_back((int64_t)rows_list.size());
+        }
+    }
+    for (int l = 1; l <= levels; ++l) {
+        for (int64_t c = 0; c < nb; ++c) {
+            const int64_t half = (int64_t)1 << (l - 1);
+            const int64_t mid = ((c >> l) << l) + half;
+            // blocks [c, mid) on the left of the middle, [mid, c] on the right
+            const int64_t c0 = c < mid ? c : mid, c1 = c < mid ? std::min(mid, nb) : c + 1;
+            const int64_t B = (int64_t)1 << b;
+            range_nodes(t, std::max((lob + c0) * B, lo0), std::min((lob + c1) * B, lo0 + n0),
+                        rows_list);
+            off.push_back((int64_t)rows_list.size());
+        }
+    }
+    const int64_t extra = (int64_t)off.size() - 1;
+    // a new node table with room for the table rows; the tree rows move over
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void* grown = nullptr;
+    if (cudaMalloc(&grown, (size_t)((t->rows + extra) * T * es)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RPYB_E_NOMEM, "device allocation of the range table failed");
+    }
+    if (cudaMemcpyAsync(grown, t->nodes, (size_t)(t->rows * T * es), cudaMemcpyDeviceToDevice,
+                        s) != cudaSuccess) {
+        rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+        cudaFree(grown);
+        return rc;
+    }
+    void* old_nodes = t->nodes;
+    // products in chunks: float64 accumulation on the device, stored once
+    // in the tree's type
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(8192, ((int64_t)1 << 30) / (T * 8)));
+    Scratch sc(nullptr, 0, s);
+    void* mem = nullptr;
+    if ((rc = sc.get((size_t)(chunk * T * 8 + chunk * 8 + 256), &mem))) {
+        cudaFree(grown);
+        return rc;
+    }
+    double* acc = static_cast<double*>(mem);
+    int64_t* d_dst = reinterpret_cast<int64_t*>(static_cast<char*>(mem) + chunk * T * 8);
+    const bool chain = chain_products_available(g);
+    std::vector<int64_t> loff, lrows, dst;
+    for (int64_t e0 = 0; e0 < extra && rc == RPYB_OK; e0 += chunk) {
+        const int64_t m = std::min(chunk, extra - e0);
+        loff.assign(m + 1, 0);
+        for (int64_t i = 0; i <= m; ++i) loff[i] = off[e0 + i] - off[e0];
+        lrows.assign(rows_list.begin() + off[e0], rows_list.begin() + off[e0 + m]);
+        dst.resize(m);
+        for (int64_t i = 0; i < m; ++i) dst[i] = t->rows + e0 + i;
+        if (chain) {
+            rc = chain_products(t->mode, g, m, acc, grown, loff, lrows, false, s);
+        } else {
+            rc = unit_rows(RPYB_F64, acc, T, T, nullptr, m, s);
+            if (!rc) rc = ordered_products(RPYB_F64, t->mode, g, m, acc, grown, loff, lrows, s);
+        }
+        if (rc) break;
+        if (cudaMemcpyAsync(d_dst, dst.data(), (size_t)m * 8, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+            break;
+        }
+        const unsigned blocks = (unsigned)std::min<int64_t>((m * T + 255) / 256, 148 * 32);
+        if (t->mode == RPYB_F64)
+            store_rows_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(grown), T, acc,
+                                                             d_dst, m);
+        else
+            store_rows_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(grown), T, acc,
+                                                            d_dst, m);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(RPYB_E_CUDA, "store_rows_kernel launch");
+        // the host vectors are reused by the next chunk: wait for the copy
+        if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "cudaStreamSynchronize");
+    }
+    if (rc) {
+        cudaStreamSynchronize(s);
+        cudaFree(grown);
+        return rc;
+    }
+    RPYB_CUDA(cudaStreamSynchronize(s));
+    cudaFree(old_nodes);
+    t->nodes = grown;
+    t->tb = b;
+    t->pre_base = t->rows;
+    t->suf_base = t->rows + n0;
+    t->dst_base = t->rows + 2 * n0;
+    t->dst_levels = levels;
+    return RPYB_OK;
+}
+
 RPYB_API int64_t rpyb_dyadic_save_size(const rpyb_dyadic_tree* t)
 {
     if (!t) return fail(RPYB_E_INVALID, "null tree");
@@ -464,6 +621,39 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* t, int64_t n_queries,
         qoff.assign(m + 1, 0);
         nodes.clear();
         for (int64_t q = 0; q < m; ++q) {
+            if (t->tb >= 0 && poff[q + 1] > poff[q]) {
+                // with the range table: pieces no finer than the leaves cover the
+                // leaf range [la, lb); across blocks it is at most four factors
+                bool coarse = true;
+                for (int64_t i = poff[q]; i < poff[q + 1]; ++i)
+                    coarse = coarse && p[i] <= R && R - p[i] <= 40;
+                if (coarse) {
+                    const int64_t i0 = poff[q], i1 = poff[q + 1] - 1;
+                    const int64_t lo0 = t->lo[0], hi0 = t->lo[0] + t->cnt[0];
+                    const int64_t la = std::max(k[i0] * ((int64_t)1 << (R - p[i0])), lo0);
+                    const int64_t lb = std::min((k[i1] + 1) * ((int64_t)1 << (R - p[i1])), hi0);
+                    const int b = t->tb;
+                    if (la < lb && (la >> b) != ((lb - 1) >> b)) {
+                        const int64_t A = la >> b, Bk = (lb - 1) >> b;
+                        const bool la_al = (la >> b) * ((int64_t)1 << b) == la;
+                        const bool lb_al = (lb >> b) * ((int64_t)1 << b) == lb;
+                        if (!la_al) nodes.push_back(t->suf_base + (la - lo0));
+                        const int64_t A1 = A + (la_al ? 0 : 1), B1 = Bk - (lb_al ? 0 : 1);
+                        if (A1 == B1) {
+                            nodes.push_back(node_row(t, b, A1));
+                        } else if (A1 < B1) {
+                            const int64_t ra = A1 - t->lo[b], rb = B1 - t->lo[b];
+                            const int l = 64 - __builtin_clzll((unsigned long long)(ra ^ rb));
+                            const int64_t nb = t->cnt[b];
+                            nodes.push_back(t->dst_base + (int64_t)(l - 1) * nb + ra);
+                            nodes.push_back(t->dst_base + (int64_t)(l - 1) * nb + rb);
+                        }
+                        if (!lb_al) nodes.push_back(t->pre_base + (lb - 1 - lo0));
+                        qoff[q + 1] = (int64_t)nodes.size();
+                        continue;
+                    }
+                }
+            }
             for (int64_t i = poff[q]; i < poff[q + 1]; ++i) {
                 int64_t row;
                 if (p[i] <= R) {

@@ -461,6 +461,21 @@ class LieIncrementStream(_StreamQueries):
         self._tree = _DyadicTree(handle, self.device)
         return self._tree
 
+    def build_range_table(self, block_log2: int = 0) -> None:
+        """Build the tree's range-product table (``rpyb_dyadic_range_table``):
+        queries spanning more than one block of leaves then multiply at most
+        four table rows instead of every dyadic piece.  Done automatically at
+        the first batch of 1024 or more queries on a tree of 4096 or more
+        leaves (``auto_range_table``)."""
+        tr = self._build_tree()
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(_lib.lib.rpyb_dyadic_range_table(tr.handle, int(block_log2), stream))
+        tr.refresh()
+        tr.range_table = True
+
+    auto_range_table = True
+
     # ------------------------------------------------------------- persistence
     def save(self, path) -> None:
         """Write the stream (events, shape, resolution, support) and its
@@ -507,6 +522,9 @@ class LieIncrementStream(_StreamQueries):
         """One rpyb_dyadic_query over clopen intervals; float64 device outputs."""
         tr = self._build_tree()
         infs = np.ascontiguousarray(infs, dtype=np.float64).reshape(-1)
+        if (self.auto_range_table and not tr.range_table and infs.shape[0] >= 1024
+                and tr.rows >= 8192):
+            self.build_range_table()
         sups = np.ascontiguousarray(sups, dtype=np.float64).reshape(-1)
         n = infs.shape[0]
         L, T = self.lie_basis.size(), self.tensor_basis.size()
@@ -756,11 +774,16 @@ class _DyadicTree:
     def __init__(self, handle, device):
         self.handle = handle
         self.device = device
+        self.range_table = False
+        self.refresh()
+
+    def refresh(self):
+        """Re-read the node table's size and address (the range table moves it)."""
         rows = ctypes.c_int64()
         top = ctypes.c_int32()
         nodes = ctypes.c_void_p()
-        _lib.check(_lib.lib.rpyb_dyadic_tree_info(handle, ctypes.byref(rows), ctypes.byref(top),
-                                                  ctypes.byref(nodes)))
+        _lib.check(_lib.lib.rpyb_dyadic_tree_info(self.handle, ctypes.byref(rows),
+                                                  ctypes.byref(top), ctypes.byref(nodes)))
         self.rows, self.top_level, self.nodes = rows.value, top.value, nodes.value
 
     def node_row(self, level: int, block: int) -> int:

@@ -408,3 +408,37 @@ def test_batched_cbh_against_the_restated_context(golden, w, d):
         lie_close(got[q], want, 1e-12)
     assert np.array_equal(got[2], lists[2][0])
     lie_close(cbh(lists[0], w, d), a.cbh(lists[0]), 1e-12)
+
+
+@pytest.mark.parametrize("dtype,n,res,lo", [(np.float64, 5000, 12, 0.0), (np.float32, 6000, 12, -0.4),
+                                            (np.float64, 3000, 13, -1.0)])
+def test_range_table_queries_equal_the_piece_products(dtype, n, res, lo):
+    """rpyb_dyadic_range_table: queries answered from the table (at most four
+    rows) equal the piece-by-piece products of the same tree: float64 trees
+    to 1e-12 (the product is only reassociated), float32 trees to 1e-6.
+    Queries include block-aligned ends, ranges inside one block, empty and
+    out-of-support ranges, supports on both sides of 0, and resolutions finer
+    than the stream's (those keep the piece path)."""
+    rng = np.random.default_rng(n + res)
+    inc = rng.normal(0, 0.02, size=(n, 3)).astype(dtype)
+    idx = np.sort(rng.uniform(lo, lo + 1.3, size=n))
+    plain = LieIncrementStream.from_increments(inc, indices=idx, width=3, depth=4, resolution=res)
+    plain.auto_range_table = False
+    table = LieIncrementStream.from_increments(inc, indices=idx, width=3, depth=4, resolution=res)
+    table.build_range_table()
+    assert table._tree.range_table and table._tree.rows == plain._build_tree().rows
+    q = np.sort(rng.uniform(lo - 0.2, lo + 1.5, size=(700, 2)), axis=1)
+    grid = np.ldexp(1.0, -res)
+    q[:100] = np.round(q[:100] / grid) * grid            # leaf-aligned ends
+    q[100:150, 1] = q[100:150, 0] + 3 * grid              # inside one block
+    q[150:160, 1] = q[150:160, 0]                          # empty
+    q[160:170] = [lo + 5.0, lo + 6.0]                      # outside the support
+    tol = 1e-12 if dtype == np.float64 else 1e-6
+    for resolution in (None, res + 3):
+        a = plain.log_signature_batch(q[:, 0], q[:, 1], resolution=resolution).cpu().numpy()
+        b = table.log_signature_batch(q[:, 0], q[:, 1], resolution=resolution).cpu().numpy()
+        scale = np.maximum(np.abs(a).max(axis=1, keepdims=True), 1e-300)
+        assert float((np.abs(a - b) / scale).max()) <= tol, resolution
+        sa = plain.signature_batch(q[:, 0], q[:, 1], resolution=resolution).cpu().numpy()
+        sb = table.signature_batch(q[:, 0], q[:, 1], resolution=resolution).cpu().numpy()
+        assert level_rel_err(sb, sa, 3, 4) <= tol
