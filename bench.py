@@ -405,6 +405,20 @@ def level_rel_err_torch(got, want, width, depth):
     return worst
 
 
+_FLUSH = {}
+
+
+def flush_l2(torch, dev):
+    """Evict L2 (126 MB): write a 256 MB buffer, then read it back so that
+    the lines left in L2 are clean and no write-back falls in the next timed
+    launch."""
+    buf = _FLUSH.get(str(dev))
+    if buf is None:
+        buf = _FLUSH[str(dev)] = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    buf.fill_(1.0)
+    buf.sum()
+
+
 def fma_sweep(dev, hbm_gbs):
     """Config-2 FMA sweep: C += A (x) B over 1024 pairs; GB/s vs HBM."""
     import torch
@@ -427,20 +441,25 @@ def fma_sweep(dev, hbm_gbs):
             for _ in range(3):
                 run()
             torch.cuda.synchronize(dev)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
+            # each launch timed alone after an L2 flush (the (2,12) float32
+            # operands, 100 MB, would otherwise stay resident in the 126 MB L2)
             reps = 10
-            e0.record()
+            ms = 0.0
             for _ in range(reps):
+                flush_l2(torch, dev)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
                 run()
-            e1.record()
-            torch.cuda.synchronize(dev)
-            ms = e0.elapsed_time(e1) / reps
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms += e0.elapsed_time(e1) / reps
             gbs = 4.0 * T * es * SWEEP_BATCH / (ms / 1e3) / 1e9
             res[f"w{w}d{d}_{name}"] = {"ms": round(ms, 4), "GB/s": round(gbs, 1),
                                        "frac_hbm": round(gbs / hbm_gbs, 3)}
             del A, B, C
     torch.cuda.empty_cache()
+    res["timing"] = "each launch timed alone by CUDA events after an L2 flush; mean of 10"
     return res
 
 
