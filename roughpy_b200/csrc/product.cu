@@ -218,7 +218,7 @@ product_kernel(const KArgs a)
 // right-factor words (r'_{p..k-2}, c) do not depend on the first, so D + V
 // loads feed D V FMAs; the top-level words of the p = k and p = 0 terms are
 // read as runs of V consecutive words.
-template <typename T, typename TR, int D, int V, int ACC = 0, int MINB = 1>
+template <typename T, typename TR, int D, int V, int ACC = 0, int MINB = 1, bool PIPE = false>
 __global__ void __launch_bounds__(kThreads, MINB)
 product_kernel_blocked(const KArgs a)
 {
@@ -274,26 +274,63 @@ product_kernel_blocked(const KArgs a)
                 // right word (r'_p..r'_{k-2}, c) = m d + c with q, m peeled from r'
                 uint32_t q = rp;
                 uint32_t m = 0;
-                for (int s = 1; s <= k - 1; ++s) {
-                    const int p = k - s;
-                    if (p <= pmax && p >= pmin) {
-                        T lv[D];
-                        T rv[V];
+                if (PIPE && pmin <= 1 && pmax >= k - 1) {
+                    // every split point 1..k-1: the loads of split s + 1 are
+                    // issued before the FMAs of split s
+                    T lv[D];
+                    TR rv[V];
+                    auto load = [&](int sd) {
+                        const int p = k - sd;
                         const T* lp = lhs + a.db[p] + q;
                         const uint32_t dp1 = (uint32_t)a.pw[p - 1];
 #pragma unroll
                         for (int u = 0; u < D; ++u) lv[u] = __ldg(lp + u * dp1);
-                        const TR* rq = rhs + a.db[s] + (int64_t)m * D + c0;
+                        const TR* rq = rhs + a.db[sd] + (int64_t)m * D + c0;
 #pragma unroll
-                        for (int j = 0; j < V; ++j) rv[j] = T(__ldg(rq + j));
+                        for (int j = 0; j < V; ++j) rv[j] = __ldg(rq + j);
+                    };
+                    auto peel = [&](int sd) {
+                        const uint32_t q2 = q / (uint32_t)D;
+                        m += (q - q2 * (uint32_t)D) * (uint32_t)a.pw[sd - 1];
+                        q = q2;
+                    };
+                    if (k >= 2) load(1);
+                    for (int sd = 1; sd <= k - 1; ++sd) {
+                        T cl[D];
+                        TR cr[V];
+#pragma unroll
+                        for (int u = 0; u < D; ++u) cl[u] = lv[u];
+#pragma unroll
+                        for (int j = 0; j < V; ++j) cr[j] = rv[j];
+                        peel(sd);
+                        if (sd + 1 <= k - 1) load(sd + 1);
 #pragma unroll
                         for (int u = 0; u < D; ++u)
 #pragma unroll
-                            for (int j = 0; j < V; ++j) acc[u][j].add(lv[u], rv[j]);
+                            for (int j = 0; j < V; ++j) acc[u][j].add(cl[u], T(cr[j]));
                     }
-                    const uint32_t q2 = q / (uint32_t)D;
-                    m += (q - q2 * (uint32_t)D) * (uint32_t)a.pw[s - 1];
-                    q = q2;
+                } else {
+                    for (int s = 1; s <= k - 1; ++s) {
+                        const int p = k - s;
+                        if (p <= pmax && p >= pmin) {
+                            T lv[D];
+                            T rv[V];
+                            const T* lp = lhs + a.db[p] + q;
+                            const uint32_t dp1 = (uint32_t)a.pw[p - 1];
+#pragma unroll
+                            for (int u = 0; u < D; ++u) lv[u] = __ldg(lp + u * dp1);
+                            const TR* rq = rhs + a.db[s] + (int64_t)m * D + c0;
+#pragma unroll
+                            for (int j = 0; j < V; ++j) rv[j] = T(__ldg(rq + j));
+#pragma unroll
+                            for (int u = 0; u < D; ++u)
+#pragma unroll
+                                for (int j = 0; j < V; ++j) acc[u][j].add(lv[u], rv[j]);
+                        }
+                        const uint32_t q2 = q / (uint32_t)D;
+                        m += (q - q2 * (uint32_t)D) * (uint32_t)a.pw[s - 1];
+                        q = q2;
+                    }
                 }
                 if (pmin <= 0 && pmax >= 0) {
                     const TR* rk = rhs + obase;
@@ -521,6 +558,17 @@ bool product_prefetch()
     return on;
 }
 
+// RPYB_PRODUCT_PIPE=0: the width-8 float32 blocked kernel walks its split
+// points without software pipelining
+bool product_pipe()
+{
+    static const bool on = [] {
+        const char* e = getenv("RPYB_PRODUCT_PIPE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 bool f32_wide_blocks()
 {
     static const bool on = [] {
@@ -590,6 +638,10 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
         RPYB_CUDA(cudaGetLastError());
         return RPYB_OK;
     }
+    // the pipelined split loop for float32 rows at width 8 (float64
+    // accumulation); measured on B200, % of HBM: (8,6) 62.8 -> 65.2,
+    // (8,5) 61.4 -> 65.7, but width 6 61.5 -> 60.6, so width 6 keeps the plain loop
+    const bool pipe = product_pipe() && sizeof(T) == 4 && ACC == 1;
     switch (a.width) {
         // last-letter blocks and resident blocks per SM (register caps) from
         // measurements on B200
@@ -603,10 +655,14 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
         case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
         case 6: product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
         case 8:
-            if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks())
-                product_kernel_blocked<T, TR, 8, 4, ACC, 2><<<grid, kThreads, 0, stream>>>(a);
-            else
+            if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks()) {
+                if (pipe)
+                    product_kernel_blocked<T, TR, 8, 4, ACC, 2, true><<<grid, kThreads, 0, stream>>>(a);
+                else
+                    product_kernel_blocked<T, TR, 8, 4, ACC, 2><<<grid, kThreads, 0, stream>>>(a);
+            } else {
                 product_kernel_blocked<T, TR, 8, 2, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+            }
             break;
         default: return fail(RPYB_E_UNSUPPORTED, "no blocked product kernel for this width");
     }
