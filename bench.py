@@ -554,7 +554,8 @@ def dyadic_queries(dev):
     depth 5, resolution 16, 100000 clopen queries with endpoints on the 2^-16
     grid; log-signatures (Chen reduction over cached dyadic nodes through the
     tree's range-product table, float64 log and Hall projection).  The tree
-    and the table are built (and timed) before the queries.  The reference's uncached recursion is estimated
+    and the table are built (and timed, as a process's second build) before
+    the queries.  The reference's uncached recursion is estimated
     from its timed two-element CBH times the exact number it would perform."""
     import torch
     from roughpy_b200.streams import LieIncrementStream
@@ -574,17 +575,26 @@ def dyadic_queries(dev):
                                                   depth=5, resolution=16, device=dev)
         warm.log_signature_batch(q[:1000, 0] / 256, q[:1000, 1] / 256)
         del warm
-        st = LieIncrementStream.from_increments(data, indices=idx, width=6, depth=5,
-                                                resolution=16, device=dev)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        st._build_tree()
-        torch.cuda.synchronize()
-        tb = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        st.build_range_table()
-        torch.cuda.synchronize()
-        tt = time.perf_counter() - t0
+        # the first full-size build of a process also pays first-use costs
+        # (measured 12-56 ms against 11-13 ms for later builds): built once
+        # untimed-in-the-value, then rebuilt and timed
+        first = {}
+        for attempt in range(2):
+            st = LieIncrementStream.from_increments(data, indices=idx, width=6, depth=5,
+                                                    resolution=16, device=dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st._build_tree()
+            torch.cuda.synchronize()
+            tb = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            st.build_range_table()
+            torch.cuda.synchronize()
+            tt = time.perf_counter() - t0
+            if attempt == 0:
+                first = {"tree_build_ms": round(tb * 1e3, 2), "range_table_ms": round(tt * 1e3, 2)}
+                del st
+                torch.cuda.empty_cache()
         st.log_signature_batch(q[:, 0], q[:, 1])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -593,7 +603,7 @@ def dyadic_queries(dev):
         tq = time.perf_counter() - t0
         lies[mode] = lie.cpu().numpy()
         res[mode] = {"tree_build_ms": round(tb * 1e3, 2), "range_table_ms": round(tt * 1e3, 2),
-                     "queries_s": round(tq, 4),
+                     "first_build": first, "queries_s": round(tq, 4),
                      "value": round(nq / tq, 1), "unit": "queries/s (wall clock, host "
                                                          "dissection included)"}
         del st
