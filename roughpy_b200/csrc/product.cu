@@ -51,6 +51,8 @@ struct KArgs {
     const int64_t* rhs_idx;
     int64_t batch;
     bool prefetch;   // L2 prefetch of the p = 0 term's streamed right words
+    int sklo, skhi;  // blocked kernels: levels computed word by word by each
+                     // row's first tile (with the level-0 rule); none if skhi < sklo
 };
 
 __device__ __forceinline__ void prefetch_l2(const void* p)
@@ -210,6 +212,52 @@ product_kernel(const KArgs a)
     }
 }
 
+// Levels sklo..skhi (at most the owned letters) and the level-0 rule of one
+// row, word by word, by the threads of the row's first tile: the same terms
+// in the same order as product_kernel, so the blocked kernels need no
+// second launch for them.
+template <typename T, typename TR, typename AccT>
+__device__ __forceinline__ void small_levels(const KArgs& a, T* __restrict__ out,
+                                             const T* __restrict__ lhs,
+                                             const TR* __restrict__ rhs,
+                                             const T* __restrict__ add, T lhs0)
+{
+    if (a.l0_write && threadIdx.x == 0) {
+        T v0 = T(0);
+        if (a.l0_base == 1) v0 = out[0];
+        else if (a.l0_base == 2) v0 = add[0];
+        v0 += T(a.l0_const);
+        if (a.l0_prod) v0 += T(a.scale0) * (lhs0 * T(__ldg(rhs)));
+        out[0] = v0;
+    }
+    int64_t w = threadIdx.x;
+    for (int k = a.sklo; k <= a.skhi; ++k) {
+        const int64_t nk = a.pw[k];
+        for (; w < nk; w += kThreads) {
+            const int64_t o = a.db[k] + w;
+            AccT acc;
+            acc.init(a.accumulate ? out[o] : T(0));
+            for (int p = k; p >= a.pmin[k]; --p) {
+                if (p > a.pmax[k]) continue;
+                const int sdeg = k - p;
+                const int64_t ds = a.pw[sdeg];
+                const int64_t li = w / ds, ri = w - li * ds;
+                const T lv = (p == 0) ? lhs0 : __ldg(lhs + a.db[p] + li);
+                acc.add(lv, T(__ldg(rhs + a.db[sdeg] + ri)));
+            }
+            T v;
+            if (a.accumulate) {
+                v = acc.value();
+            } else {
+                v = T(a.scale[k]) * acc.value();
+                if (add) v += add[o];
+            }
+            out[o] = v;
+        }
+        w -= nk;
+    }
+}
+
 // Blocked variant for output levels k >= 2 (one owned last letter).  A thread owns the D x V words
 //   u d^(k-1) + r' d + c0 + j    (u < D first letters, j < V last letters)
 // for one middle part r' (k-2 letters) and one block c0 .. c0+V-1 of last
@@ -238,6 +286,7 @@ product_kernel_blocked(const KArgs a)
             a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
         const T lhs0 = (a.lhs0_from_mem ? __ldg(lhs) : T(0)) + T(a.lhs0_add);
         const T rhs0 = T(__ldg(rhs));
+        if (blockIdx.x == 0) small_levels<T, TR, AccT>(a, out, lhs, rhs, add, lhs0);
 
         for (int64_t f = f_begin + threadIdx.x; f < f_end; f += kThreads) {
             int k = a.klo;
@@ -387,6 +436,7 @@ product_kernel_blocked_l(const KArgs a)
             a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
         const T lhs0 = (a.lhs0_from_mem ? __ldg(lhs) : T(0)) + T(a.lhs0_add);
         const T rhs0 = T(__ldg(rhs));
+        if (blockIdx.x == 0) small_levels<T, TR, AccT>(a, out, lhs, rhs, add, lhs0);
 
         for (int64_t f = f_begin + threadIdx.x; f < f_end; f += kThreads) {
             int k = a.klo;
@@ -682,17 +732,9 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
     const int L = blocked_enabled() ? blocked_l(g.width) : 0;
     const int kb = std::max(L + 1, spec.klo);
     if (L == 0 || spec.khi < kb) return launch_levels(dtype, g, spec, rows, stream, false);
-    // levels 0..L (and the level-0 rule) by the suffix kernel, the rest blocked
-    int rc;
-    if (spec.klo <= L || spec.l0_write) {
-        ProductSpec lo = spec;
-        lo.khi = std::min(spec.khi, L);
-        if ((rc = launch_levels(dtype, g, lo, rows, stream, false))) return rc;
-    }
-    ProductSpec hi = spec;
-    hi.klo = kb;
-    hi.l0_write = false;
-    return launch_levels(dtype, g, hi, rows, stream, true);
+    // one blocked launch: levels kb..khi by units, levels klo..L and the
+    // level-0 rule word by word in each row's first tile
+    return launch_levels(dtype, g, spec, rows, stream, true);
 }
 
 static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
@@ -702,6 +744,14 @@ static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
     a.width = g.width;
     a.klo = std::max(1, spec.klo);
     a.khi = spec.khi;
+    a.sklo = 1;
+    a.skhi = 0;
+    if (blocked) {
+        const int Lb = blocked_l(g.width);
+        a.sklo = a.klo;
+        a.skhi = std::min(spec.khi, Lb);
+        a.klo = std::max(Lb + 1, spec.klo);
+    }
     for (int i = 0; i <= kMaxDepth + 1; ++i) a.db[i] = g.db[i];
     for (int i = 0; i <= kMaxDepth; ++i) a.pw[i] = g.pw[i];
     int64_t f = 0;

@@ -66,8 +66,10 @@ int upload(const std::vector<E>& h, const E** out)
 // The packed form of a CSR map for lie_project_kernel: rows sorted by entry
 // count (most first, stably) in groups of 32, each group padded to its
 // longest row with zero entries and stored lane-interleaved (entry j of lane
-// l at 32 j + l from the group's offset); an entry is column | value id << 16.
-// False when a column or the number of distinct values does not fit 16 bits.
+// l at 32 j + l from the group's offset); an entry is 8 * column | value id
+// << 19 (the byte offset of a float64 word of the row, so the kernel's
+// gather needs no scaling).  False when a column does not fit 16 bits or
+// the number of distinct values 13 bits.
 bool pack_csr(const std::vector<int64_t>& hp, const std::vector<int64_t>& hi,
               const std::vector<double>& hv, int64_t n_rows, int64_t n_cols,
               std::vector<uint32_t>& goff, std::vector<uint32_t>& ent,
@@ -81,7 +83,7 @@ bool pack_csr(const std::vector<int64_t>& hp, const std::vector<int64_t>& hi,
         std::memcpy(&bits, &v, sizeof bits);
         auto it = ids.find(bits);
         if (it == ids.end()) {
-            if (tab.size() > 0xffff) return false;
+            if (tab.size() > 0x1fff) return false;
             it = ids.emplace(bits, (uint32_t)tab.size()).first;
             tab.push_back(v);
         }
@@ -108,14 +110,14 @@ bool pack_csr(const std::vector<int64_t>& hp, const std::vector<int64_t>& hi,
         }
         for (int64_t j = 0; j < len; ++j)
             for (int l = 0; l < 32; ++l) {
-                uint32_t e = zero_id << 16;
+                uint32_t e = zero_id << 19;
                 if (g * 32 + l < n_rows) {
                     const int64_t r = order[g * 32 + l];
                     if (j < hp[r + 1] - hp[r]) {
                         const int64_t k = hp[r] + j;
                         uint32_t vid;
                         if (hi[k] < 0 || hi[k] >= n_cols || !id_of(hv[k], &vid)) return false;
-                        e = (uint32_t)hi[k] | (vid << 16);
+                        e = ((uint32_t)hi[k] << 3) | (vid << 19);
                     }
                 }
                 ent.push_back(e);
@@ -227,17 +229,19 @@ struct ProjArgs {
 template <typename T>
 size_t proj_smem_bytes(const ProjArgs& a)
 {
-    return (size_t)(a.ntab * 8 + a.n_cols * (int64_t)sizeof(T) + (a.groups + 1) * 4 + a.slots * 4);
+    const int64_t xs_bytes = (a.n_cols * (int64_t)sizeof(T) + 15) / 16 * 16;
+    return (size_t)(xs_bytes + a.ntab * 8 + (a.groups + 1) * 4 + a.slots * 4);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kProjThreads, 1)
 lie_project_kernel(const ProjArgs a, T* __restrict__ y, const T* __restrict__ x)
 {
+    // the row first, so an entry's byte offset addresses its word directly
     extern __shared__ __align__(16) unsigned char proj_smem[];
-    double* tab = reinterpret_cast<double*>(proj_smem);
-    T* xs = reinterpret_cast<T*>(tab + a.ntab);
-    uint32_t* goff = reinterpret_cast<uint32_t*>(xs + a.n_cols);
+    T* xs = reinterpret_cast<T*>(proj_smem);
+    double* tab = reinterpret_cast<double*>(proj_smem + (a.n_cols * (int64_t)sizeof(T) + 15) / 16 * 16);
+    uint32_t* goff = reinterpret_cast<uint32_t*>(tab + a.ntab);
     uint32_t* ent = goff + a.groups + 1;
     const int tid = (int)threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = (int)blockDim.x >> 5;
@@ -277,7 +281,10 @@ lie_project_kernel(const ProjArgs a, T* __restrict__ y, const T* __restrict__ x)
 #pragma unroll 4
             for (uint32_t k = goff[g] + lane; k < e1; k += 32) {
                 const uint32_t w = ent[k];
-                acc = fma(tab[w >> 16], (double)xs[w & 0xffffu], acc);
+                const uint32_t off = w & 0x7ffffu;   // 8 * column
+                const T xv = *reinterpret_cast<const T*>(
+                    proj_smem + (sizeof(T) == 8 ? off : off >> 1));
+                acc = fma(tab[w >> 19], (double)xv, acc);
             }
             const uint32_t row = __ldg(a.perm + g * 32 + lane);
             if (row != 0xffffffffu) yr[row] = (T)acc;

@@ -23,10 +23,10 @@ struct LieMapsDev {
     const int64_t* t2l_idx = nullptr;
     const double* t2l_val = nullptr;
     // t2l packed for the shared-memory projection kernel (null when a column
-    // or the number of distinct values does not fit 16 bits).  Rows sorted by
+    // does not fit 16 bits or the number of distinct values 13 bits).  Rows sorted by
     // entry count, in groups of 32 (one per warp lane), each group padded to
     // its longest row; entry j of lane l of group g is t2l_ent[t2l_goff[g] +
-    // 32 j + l] = column | (value id << 16), the distinct values (and a zero
+    // 32 j + l] = 8 * column | (value id << 19), the distinct values (and a zero
     // for the padding) in t2l_tab; t2l_perm[32 g + l] is the lane's row, or
     // 0xffffffff past the last row.
     const uint32_t* t2l_goff = nullptr;   // groups + 1
