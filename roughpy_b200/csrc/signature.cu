@@ -790,8 +790,22 @@ signature_kernel_split(const SigArgs a)
                 products(x, accx, accm);
             }
 
-            // the chunk's increment sum joins the fold period's sum X
-            if (lane < D) {
+            // the chunk's increment sum joins the fold period's sum X: with
+            // D <= 8 each letter is summed by 32 / 8 = 4 lanes over a quarter
+            // of the steps, then the quarters are added by shuffles
+            if constexpr (D <= 8) {
+                const int letter = lane & 7, quarter = lane >> 3;
+                double part = 0.0;
+                if (letter < D) {
+                    const int j0 = quarter * (kChunk / 4);
+#pragma unroll
+                    for (int jj = j0; jj < j0 + kChunk / 4; ++jj)
+                        if (jj < nsteps) part += x64[jj * D + letter];
+                }
+                part += __shfl_xor_sync(0xffffffffu, part, 8);
+                part += __shfl_xor_sync(0xffffffffu, part, 16);
+                if (lane < D) xsum[lane] += part;
+            } else if (lane < D) {
                 double sum = xsum[lane];
                 for (int jj = 0; jj < nsteps; ++jj) sum += x64[jj * D + lane];
                 xsum[lane] = sum;
