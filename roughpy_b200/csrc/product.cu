@@ -1,21 +1,23 @@
-// Batched truncated free-tensor product kernel (sm_100a).
+// Batched truncated free-tensor product kernels (sm_100a).
 //
 // Work decomposition.  Output level k (k >= 1) holds d^k words; write a word
 // as w = u * d^(k-1) + r with u its first letter.  For every split p >= 1 the
 // right factor R_{k-p}[w mod d^(k-p)] = R_{k-p}[r mod d^(k-p)] does not depend
-// on u, so one thread owns a suffix r and produces the d words
-// {u * d^(k-1) + r : u < d}: each right-factor word is loaded once and reused
-// d times from a register, each left-factor word L_p[u d^(p-1) + r / d^(k-p)]
-// is a warp broadcast for small p, and the top-level streams
-// (L_k, R_k, old out_k) are coalesced across consecutive r.  The (level, r)
-// pairs of all output levels are flattened into one index space that is cut
-// into tiles of TILE_R suffixes; blockIdx.x walks tiles of one row so that
-// a row's lower levels stay hot in L2, blockIdx.y walks rows.
+// on u.  The suffix kernel (product_kernel) lets one thread own a suffix r and
+// produce the d words {u * d^(k-1) + r : u < d}; the blocked kernels (widths
+// 2..6 and 8, the default) let a thread own the d first letters times a block
+// of last letters, so that a split point's left words are shared by the
+// block and its right words by the first letters.  The top-level streams
+// (L_k, R_k, old out_k) are coalesced across consecutive units.  The (level,
+// unit) pairs of all output levels are flattened into one index space that
+// is cut into tiles; blockIdx.x walks tiles of one row so that a row's lower
+// levels stay hot in L2, blockIdx.y walks rows.
 //
 // Arithmetic.  float64: the terms are added in the reference order (lhs
-// degree from high to low, free_tensor_fma.hpp:31-46) with FMA.  float32:
-// every term is formed with an exact two-product and accumulated in a
-// double-float (hi, lo) pair with two-sum, rounded once at the end.
+// degree from high to low, free_tensor_fma.hpp:31-46) with FMA.  float32: by
+// default every product of two float32 words (exact in float64) is
+// accumulated in float64 and rounded once; a double-float pair or plain
+// float32 accumulation can be selected (RPYB_F32_ACC).
 #include "product.cuh"
 
 #include <algorithm>
