@@ -375,49 +375,60 @@ RPYB_API int rpyb_dyadic_range_table(rpyb_dyadic_tree* t, int32_t block_log2, vo
         return rc;
     }
     void* old_nodes = t->nodes;
-    // products in chunks: float64 accumulation on the device, stored once
-    // in the tree's type
+    // products in chunks, accumulated in float64 on the device and rounded
+    // once to the tree's type
     const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(8192, ((int64_t)1 << 30) / (T * 8)));
-    Scratch sc(nullptr, 0, s);
-    void* mem = nullptr;
-    if ((rc = sc.get((size_t)(chunk * T * 8 + chunk * 8 + 256), &mem))) {
-        cudaFree(grown);
-        return rc;
-    }
-    double* acc = static_cast<double*>(mem);
-    int64_t* d_dst = reinterpret_cast<int64_t*>(static_cast<char*>(mem) + chunk * T * 8);
     const bool chain = chain_products_available(g);
     std::vector<int64_t> loff, lrows, dst;
-    for (int64_t e0 = 0; e0 < extra && rc == RPYB_OK; e0 += chunk) {
-        const int64_t m = std::min(chunk, extra - e0);
-        loff.assign(m + 1, 0);
-        for (int64_t i = 0; i <= m; ++i) loff[i] = off[e0 + i] - off[e0];
-        lrows.assign(rows_list.begin() + off[e0], rows_list.begin() + off[e0 + m]);
-        dst.resize(m);
-        for (int64_t i = 0; i < m; ++i) dst[i] = t->rows + e0 + i;
-        if (chain) {
-            rc = chain_products(t->mode, g, m, acc, grown, loff, lrows, false, s);
-        } else {
+    if (chain) {
+        // the chain kernel writes the table rows straight into the grown
+        // node table; its index lists are copied when the call returns, so
+        // the host prepares the next chunk while the device runs this one
+        for (int64_t e0 = 0; e0 < extra && rc == RPYB_OK; e0 += chunk) {
+            const int64_t m = std::min(chunk, extra - e0);
+            loff.assign(m + 1, 0);
+            for (int64_t i = 0; i <= m; ++i) loff[i] = off[e0 + i] - off[e0];
+            lrows.assign(rows_list.begin() + off[e0], rows_list.begin() + off[e0 + m]);
+            dst.resize(m);
+            for (int64_t i = 0; i < m; ++i) dst[i] = t->rows + e0 + i;
+            rc = chain_products_into(t->mode, g, m, grown, loff, lrows, dst, s);
+        }
+    } else {
+        Scratch sc(nullptr, 0, s);
+        void* mem = nullptr;
+        if ((rc = sc.get((size_t)(chunk * T * 8 + chunk * 8 + 256), &mem))) {
+            cudaFree(grown);
+            return rc;
+        }
+        double* acc = static_cast<double*>(mem);
+        int64_t* d_dst = reinterpret_cast<int64_t*>(static_cast<char*>(mem) + chunk * T * 8);
+        for (int64_t e0 = 0; e0 < extra && rc == RPYB_OK; e0 += chunk) {
+            const int64_t m = std::min(chunk, extra - e0);
+            loff.assign(m + 1, 0);
+            for (int64_t i = 0; i <= m; ++i) loff[i] = off[e0 + i] - off[e0];
+            lrows.assign(rows_list.begin() + off[e0], rows_list.begin() + off[e0 + m]);
+            dst.resize(m);
+            for (int64_t i = 0; i < m; ++i) dst[i] = t->rows + e0 + i;
             rc = unit_rows(RPYB_F64, acc, T, T, nullptr, m, s);
             if (!rc) rc = ordered_products(RPYB_F64, t->mode, g, m, acc, grown, loff, lrows, s);
+            if (rc) break;
+            if (cudaMemcpyAsync(d_dst, dst.data(), (size_t)m * 8, cudaMemcpyHostToDevice, s) !=
+                cudaSuccess) {
+                rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+                break;
+            }
+            const unsigned blocks = (unsigned)std::min<int64_t>((m * T + 255) / 256, 148 * 32);
+            if (t->mode == RPYB_F64)
+                store_rows_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(grown), T,
+                                                                 acc, d_dst, m);
+            else
+                store_rows_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(grown), T,
+                                                                acc, d_dst, m);
+            if (cudaGetLastError() != cudaSuccess) rc = fail(RPYB_E_CUDA, "store_rows_kernel launch");
+            // the host vectors are reused by the next chunk: wait for the copy
+            if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
+                rc = cuda_fail(cudaGetLastError(), "cudaStreamSynchronize");
         }
-        if (rc) break;
-        if (cudaMemcpyAsync(d_dst, dst.data(), (size_t)m * 8, cudaMemcpyHostToDevice, s) !=
-            cudaSuccess) {
-            rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
-            break;
-        }
-        const unsigned blocks = (unsigned)std::min<int64_t>((m * T + 255) / 256, 148 * 32);
-        if (t->mode == RPYB_F64)
-            store_rows_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(grown), T, acc,
-                                                             d_dst, m);
-        else
-            store_rows_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(grown), T, acc,
-                                                            d_dst, m);
-        if (cudaGetLastError() != cudaSuccess) rc = fail(RPYB_E_CUDA, "store_rows_kernel launch");
-        // the host vectors are reused by the next chunk: wait for the copy
-        if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
-            rc = cuda_fail(cudaGetLastError(), "cudaStreamSynchronize");
     }
     if (rc) {
         cudaStreamSynchronize(s);

@@ -335,6 +335,8 @@ struct ChainArgs {
     const void* src = nullptr;         // [*, T] factors (float or double)
     double* acc = nullptr;             // [n, T] out
     int log_out = 0;                   // write log(product) instead of the product
+    void* dst = nullptr;               // instead of acc: rows dst_rows[q] of this
+    const int64_t* dst_rows = nullptr; // [*, T] array of the factors' type
 };
 
 constexpr int kChainThreads = 512;
@@ -428,8 +430,13 @@ chain_products_kernel(const ChainArgs a)
     for (int64_t q = blockIdx.x; q < a.n; q += gridDim.x) {
         const int64_t o0 = a.off[q], o1 = a.off[q + 1];
         double* accq = a.acc + q * a.T;
+        TS* dstq = a.dst ? static_cast<TS*>(a.dst) + a.dst_rows[q] * a.T : nullptr;
         if (o0 == o1) {   // the unit, or its log
-            for (int64_t i = tid; i < a.T; i += B) accq[i] = (i == 0 && !a.log_out) ? 1.0 : 0.0;
+            for (int64_t i = tid; i < a.T; i += B) {
+                const double v = (i == 0 && !a.log_out) ? 1.0 : 0.0;
+                if (dstq) dstq[i] = (TS)v;
+                else accq[i] = v;
+            }
             continue;
         }
         double* cur = lo0;
@@ -551,14 +558,26 @@ chain_products_kernel(const ChainArgs a)
             __syncthreads();
             cur = rc;
         }
-        for (int64_t i = tid; i < TL; i += B) accq[i] = cur[i];
+        if (dstq) {
+            // straight into the factors' array, rounded once to its type
+            for (int64_t i = tid; i < TL; i += B) dstq[i] = (TS)cur[i];
 #pragma unroll
-        for (int t = 0; t < TU; ++t)
-            if (town[t])
+            for (int t = 0; t < TU; ++t)
+                if (town[t])
 #pragma unroll
-                for (int u = 0; u < D; ++u)
+                    for (int u = 0; u < D; ++u)
 #pragma unroll
-                    for (int j = 0; j < V; ++j) accq[tbase[t] + u * tdk1 + j] = top[t][u][j];
+                        for (int j = 0; j < V; ++j) dstq[tbase[t] + u * tdk1 + j] = (TS)top[t][u][j];
+        } else {
+            for (int64_t i = tid; i < TL; i += B) accq[i] = cur[i];
+#pragma unroll
+            for (int t = 0; t < TU; ++t)
+                if (town[t])
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j) accq[tbase[t] + u * tdk1 + j] = top[t][u][j];
+        }
     }
 }
 
@@ -630,13 +649,33 @@ bool chain_products_available(const Geometry& g)
     return chain_tu(g) > 0 && 3 * g.db[g.depth] * 8 <= kChainSmemLimit;
 }
 
+static int chain_launch(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
+                        const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                        bool log_out, void* dst, const std::vector<int64_t>* dst_rows,
+                        cudaStream_t s);
+
 int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                    const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
                    bool log_out, cudaStream_t s)
 {
+    return chain_launch(src_mode, g, n, acc, src, off, src_rows, log_out, nullptr, nullptr, s);
+}
+
+int chain_products_into(int src_mode, const Geometry& g, int64_t n, void* nodes,
+                        const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                        const std::vector<int64_t>& dst_rows, cudaStream_t s)
+{
+    return chain_launch(src_mode, g, n, nullptr, nodes, off, src_rows, false, nodes, &dst_rows, s);
+}
+
+static int chain_launch(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
+                        const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                        bool log_out, void* dst, const std::vector<int64_t>* dst_rows,
+                        cudaStream_t s)
+{
     if (n == 0) return RPYB_OK;
     if (!chain_products_available(g)) return fail(RPYB_E_UNSUPPORTED, "no chain kernel for this shape");
-    if (off[n] == 0) {
+    if (off[n] == 0 && !dst) {
         if (log_out) {
             RPYB_CUDA(cudaMemsetAsync(acc, 0, (size_t)(n * g.size() * 8), s));
             return RPYB_OK;
@@ -662,6 +701,7 @@ int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, cons
     // offsets and rows in one upload
     std::vector<int64_t> packed(off.begin(), off.begin() + n + 1);
     packed.insert(packed.end(), src_rows.begin(), src_rows.begin() + off[n]);
+    if (dst) packed.insert(packed.end(), dst_rows->begin(), dst_rows->begin() + n);
     Scratch sc(nullptr, 0, s);
     void* mem = nullptr;
     int rc;
@@ -673,6 +713,8 @@ int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, cons
     a.src = src;
     a.acc = acc;
     a.log_out = log_out ? 1 : 0;
+    a.dst = dst;
+    a.dst_rows = dst ? d + n + 1 + off[n] : nullptr;
     const size_t smem = (size_t)((log_out ? 3 : 2) * g.db[g.depth] * 8);
     const unsigned grid = (unsigned)std::min<int64_t>(n, 1 << 20);
     ChainFn fn = src_mode == RPYB_F64 ? chain_fn<double>(g.width, g.depth, tu)

@@ -66,6 +66,13 @@ bool chain_products_available(const Geometry& g);
 int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                    const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
                    bool log_out, cudaStream_t s);
+// The same products (float64 accumulation) written straight into rows
+// dst_rows[i] of `nodes`, the [*, T] array (of src_mode's type) that also
+// holds the factors; the destination rows must not be factors of the call.
+// The index lists are copied before the call returns.
+int chain_products_into(int src_mode, const Geometry& g, int64_t n, void* nodes,
+                        const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                        const std::vector<int64_t>& dst_rows, cudaStream_t s);
 
 // Bytes of scratch finish_queries needs for up to `n` rows.
 size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n);
