@@ -683,12 +683,24 @@ RPYB_API int rpyb_dyadic_query(const rpyb_dyadic_tree* t, int64_t n_queries,
             qoff[q + 1] = (int64_t)nodes.size();
         }
         const bool chain = chain_products_available(g);
+        double* lsq = out_logsig ? out_logsig + q0 * ld_logsig : nullptr;
+        if (chain && chain_lie_available(g, *t->maps)) {
+            // chain products, log and Hall projection in one kernel
+            int64_t ld_lie = 0;
+            double* lie = finish_lie_rows(g, t->maps->lie_dim, m, fin_mem, lsq, ld_logsig, &ld_lie);
+            if ((rc = chain_products_lie(t->mode, g, m, t->nodes, qoff, nodes, *t->maps, lie,
+                                         ld_lie, s)) ||
+                (rc = finish_queries(g, *t->maps, m, acc, true, lsq, ld_logsig,
+                                     out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig, fin_mem,
+                                     fin, s, true)))
+                return rc;
+            continue;
+        }
         if ((rc = chain ? chain_products(t->mode, g, m, acc, t->nodes, qoff, nodes, true, s)
                         : (unit_rows(RPYB_F64, acc, T, T, nullptr, m, s) ||
                            ordered_products(RPYB_F64, t->mode, g, m, acc, t->nodes, qoff, nodes,
                                             s))) ||
-            (rc = finish_queries(g, *t->maps, m, acc, chain,
-                                 out_logsig ? out_logsig + q0 * ld_logsig : nullptr, ld_logsig,
+            (rc = finish_queries(g, *t->maps, m, acc, chain, lsq, ld_logsig,
                                  out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig, fin_mem, fin,
                                  s)))
             return rc;

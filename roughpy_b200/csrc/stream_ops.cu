@@ -337,6 +337,15 @@ struct ChainArgs {
     int log_out = 0;                   // write log(product) instead of the product
     void* dst = nullptr;               // instead of acc: rows dst_rows[q] of this
     const int64_t* dst_rows = nullptr; // [*, T] array of the factors' type
+    // log_out with lie != null: the block projects its log onto the Hall
+    // basis through the packed t2l map and writes lie[q * ld_lie + row]
+    // instead of the log tensor
+    double* lie = nullptr;
+    int64_t ld_lie = 0, lie_dim = 0, pgroups = 0;
+    const uint32_t* pgoff = nullptr;
+    const uint32_t* pent = nullptr;
+    const uint32_t* pperm = nullptr;
+    const double* ptab = nullptr;
 };
 
 constexpr int kChainThreads = 512;
@@ -429,8 +438,12 @@ chain_products_kernel(const ChainArgs a)
 
     for (int64_t q = blockIdx.x; q < a.n; q += gridDim.x) {
         const int64_t o0 = a.off[q], o1 = a.off[q + 1];
-        double* accq = a.acc + q * a.T;
+        double* accq = a.acc ? a.acc + q * a.T : nullptr;
         TS* dstq = a.dst ? static_cast<TS*>(a.dst) + a.dst_rows[q] * a.T : nullptr;
+        if (o0 == o1 && a.lie) {   // the log of the unit: zero coordinates
+            for (int64_t r = tid; r < a.lie_dim; r += B) a.lie[q * a.ld_lie + r] = 0.0;
+            continue;
+        }
         if (o0 == o1) {   // the unit, or its log
             for (int64_t i = tid; i < a.T; i += B) {
                 const double v = (i == 0 && !a.log_out) ? 1.0 : 0.0;
@@ -558,6 +571,37 @@ chain_products_kernel(const ChainArgs a)
             __syncthreads();
             cur = rc;
         }
+        if (a.lie) {
+            // the whole log into shared memory (after the three log
+            // buffers), then one warp per group of 32 Lie rows; an entry is
+            // 8 * column | value id << 19 (see pack_csr)
+            double* xs = lo0 + 3 * TL;
+            for (int64_t i = tid; i < TL; i += B) xs[i] = cur[i];
+#pragma unroll
+            for (int t = 0; t < TU; ++t)
+                if (town[t])
+#pragma unroll
+                    for (int u = 0; u < D; ++u)
+#pragma unroll
+                        for (int j = 0; j < V; ++j) xs[tbase[t] + u * tdk1 + j] = top[t][u][j];
+            __syncthreads();
+            const unsigned char* xb = reinterpret_cast<const unsigned char*>(xs);
+            const int lane = tid & 31, nw = B >> 5;
+            double* yq = a.lie + q * a.ld_lie;
+            for (int64_t gi = tid >> 5; gi < a.pgroups; gi += nw) {
+                double accp = 0.0;
+                const uint32_t e1 = __ldg(a.pgoff + gi + 1);
+#pragma unroll 4
+                for (uint32_t k = __ldg(a.pgoff + gi) + lane; k < e1; k += 32) {
+                    const uint32_t w = __ldg(a.pent + k);
+                    accp = fma(__ldg(a.ptab + (w >> 19)),
+                               *reinterpret_cast<const double*>(xb + (w & 0x7ffffu)), accp);
+                }
+                const uint32_t row = __ldg(a.pperm + gi * 32 + lane);
+                if (row != 0xffffffffu) yq[row] = accp;
+            }
+            continue;
+        }
         if (dstq) {
             // straight into the factors' array, rounded once to its type
             for (int64_t i = tid; i < TL; i += B) dstq[i] = (TS)cur[i];
@@ -652,7 +696,8 @@ bool chain_products_available(const Geometry& g)
 static int chain_launch(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                         const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
                         bool log_out, void* dst, const std::vector<int64_t>* dst_rows,
-                        cudaStream_t s);
+                        cudaStream_t s, const LieMapsDev* maps = nullptr, double* lie = nullptr,
+                        int64_t ld_lie = 0);
 
 int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                    const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
@@ -668,13 +713,33 @@ int chain_products_into(int src_mode, const Geometry& g, int64_t n, void* nodes,
     return chain_launch(src_mode, g, n, nullptr, nodes, off, src_rows, false, nodes, &dst_rows, s);
 }
 
+bool chain_lie_available(const Geometry& g, const LieMapsDev& maps)
+{
+    return chain_products_available(g) && maps.t2l_ent &&
+           (size_t)(3 * g.db[g.depth] + g.size()) * 8 <= (size_t)kChainSmemLimit;
+}
+
+int chain_products_lie(int src_mode, const Geometry& g, int64_t n, const void* src,
+                       const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                       const LieMapsDev& maps, double* lie, int64_t ld_lie, cudaStream_t s)
+{
+    if (!chain_lie_available(g, maps)) return fail(RPYB_E_UNSUPPORTED, "no fused projection for this shape");
+    return chain_launch(src_mode, g, n, nullptr, src, off, src_rows, true, nullptr, nullptr, s,
+                        &maps, lie, ld_lie);
+}
+
 static int chain_launch(int src_mode, const Geometry& g, int64_t n, double* acc, const void* src,
                         const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
                         bool log_out, void* dst, const std::vector<int64_t>* dst_rows,
-                        cudaStream_t s)
+                        cudaStream_t s, const LieMapsDev* maps, double* lie, int64_t ld_lie)
 {
     if (n == 0) return RPYB_OK;
     if (!chain_products_available(g)) return fail(RPYB_E_UNSUPPORTED, "no chain kernel for this shape");
+    if (off[n] == 0 && lie) {
+        RPYB_CUDA(cudaMemset2DAsync(lie, (size_t)ld_lie * 8, 0, (size_t)maps->lie_dim * 8,
+                                    (size_t)n, s));
+        return RPYB_OK;
+    }
     if (off[n] == 0 && !dst) {
         if (log_out) {
             RPYB_CUDA(cudaMemsetAsync(acc, 0, (size_t)(n * g.size() * 8), s));
@@ -715,7 +780,18 @@ static int chain_launch(int src_mode, const Geometry& g, int64_t n, double* acc,
     a.log_out = log_out ? 1 : 0;
     a.dst = dst;
     a.dst_rows = dst ? d + n + 1 + off[n] : nullptr;
-    const size_t smem = (size_t)((log_out ? 3 : 2) * g.db[g.depth] * 8);
+    if (lie) {
+        a.lie = lie;
+        a.ld_lie = ld_lie;
+        a.lie_dim = maps->lie_dim;
+        a.pgroups = maps->t2l_groups;
+        a.pgoff = maps->t2l_goff;
+        a.pent = maps->t2l_ent;
+        a.pperm = maps->t2l_perm;
+        a.ptab = maps->t2l_tab;
+    }
+    const size_t smem =
+        (size_t)((log_out ? 3 : 2) * g.db[g.depth] * 8) + (lie ? (size_t)g.size() * 8 : 0);
     const unsigned grid = (unsigned)std::min<int64_t>(n, 1 << 20);
     ChainFn fn = src_mode == RPYB_F64 ? chain_fn<double>(g.width, g.depth, tu)
                                       : chain_fn<float>(g.width, g.depth, tu);
@@ -885,9 +961,20 @@ size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n)
     return buf + lbuf + (size_t)std::max<int64_t>(std::max(log_ws, exp_ws), 1);
 }
 
+double* finish_lie_rows(const Geometry& g, int64_t lie_dim, int64_t m, void* scratch,
+                        double* out_logsig, int64_t ld_logsig, int64_t* ld_lie)
+{
+    (void)lie_dim;
+    *ld_lie = out_logsig ? ld_logsig : lie_dim;
+    if (out_logsig) return out_logsig;
+    const size_t buf = (size_t)((m * g.size() * 8 + 255) / 256 * 256);
+    return reinterpret_cast<double*>(static_cast<char*>(scratch) + buf);
+}
+
 int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double* acc,
                    bool acc_is_log, double* out_logsig, int64_t ld_logsig, double* out_sig,
-                   int64_t ld_sig, void* scratch, size_t scratch_bytes, cudaStream_t s)
+                   int64_t ld_sig, void* scratch, size_t scratch_bytes, cudaStream_t s,
+                   bool lie_ready)
 {
     if (m <= 0) return RPYB_OK;
     const int64_t T = g.size(), L = maps.lie_dim;
@@ -895,21 +982,23 @@ int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double*
     const size_t lbuf = (size_t)((m * L * 8 + 255) / 256 * 256);
     if (scratch_bytes < buf + lbuf + 1) return fail(RPYB_E_INVALID, "query scratch too small");
     double* tmp = static_cast<double*>(scratch);
-    double* lie_tmp = reinterpret_cast<double*>(static_cast<char*>(scratch) + buf);
     void* ws = static_cast<char*>(scratch) + buf + lbuf;
     const size_t wsb = scratch_bytes - buf - lbuf;
     int rc;
-    // log in float64 (its incoming out[0] must be zero), then tensor -> Lie
-    const double* logt = acc;
-    if (!acc_is_log) {
-        RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
-        if ((rc = rpyb_ft_log(RPYB_F64, g.width, g.depth, m, tmp, acc, T, T, -1, -1, ws, wsb, s)))
-            return rc;
-        logt = tmp;
+    int64_t ld_lie = 0;
+    double* lie = finish_lie_rows(g, L, m, scratch, out_logsig, ld_logsig, &ld_lie);
+    if (!lie_ready) {
+        // log in float64 (its incoming out[0] must be zero), then tensor -> Lie
+        const double* logt = acc;
+        if (!acc_is_log) {
+            RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));
+            if ((rc = rpyb_ft_log(RPYB_F64, g.width, g.depth, m, tmp, acc, T, T, -1, -1, ws, wsb,
+                                  s)))
+                return rc;
+            logt = tmp;
+        }
+        if ((rc = lie_project(RPYB_F64, g, maps, m, lie, ld_lie, logt, T, s))) return rc;
     }
-    double* lie = out_logsig ? out_logsig : lie_tmp;
-    const int64_t ld_lie = out_logsig ? ld_logsig : L;
-    if ((rc = lie_project(RPYB_F64, g, maps, m, lie, ld_lie, logt, T, s))) return rc;
     if (out_sig) {
         // algebra/src/context.cpp:156-159: exp(lie_to_tensor(log_signature))
         RPYB_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(m * T * 8), s));

@@ -73,6 +73,13 @@ int chain_products(int src_mode, const Geometry& g, int64_t n, double* acc, cons
 int chain_products_into(int src_mode, const Geometry& g, int64_t n, void* nodes,
                         const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
                         const std::vector<int64_t>& dst_rows, cudaStream_t s);
+// log(product) projected onto the Hall basis inside the chain kernel (the
+// log never leaves the SM): Lie coordinates to lie[i * ld_lie + r].  Needs
+// the packed t2l map and room for the whole log in shared memory.
+bool chain_lie_available(const Geometry& g, const LieMapsDev& maps);
+int chain_products_lie(int src_mode, const Geometry& g, int64_t n, const void* src,
+                       const std::vector<int64_t>& off, const std::vector<int64_t>& src_rows,
+                       const LieMapsDev& maps, double* lie, int64_t ld_lie, cudaStream_t s);
 
 // Bytes of scratch finish_queries needs for up to `n` rows.
 size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n);
@@ -82,7 +89,13 @@ size_t finish_scratch_bytes(const Geometry& g, int64_t lie_dim, int64_t n);
 // exp(l2t(logsig)) into out_sig (either may be null).  Scratch from `scratch`.
 int finish_queries(const Geometry& g, const LieMapsDev& maps, int64_t m, double* acc,
                    bool acc_is_log, double* out_logsig, int64_t ld_logsig, double* out_sig,
-                   int64_t ld_sig, void* scratch, size_t scratch_bytes, cudaStream_t s);
+                   int64_t ld_sig, void* scratch, size_t scratch_bytes, cudaStream_t s,
+                   bool lie_ready = false);
+// Where finish_queries keeps the m rows of Lie coordinates (out_logsig, or
+// its scratch), with their stride; lie_ready = true means the caller wrote
+// them there already (chain_products_lie) and only out_sig remains.
+double* finish_lie_rows(const Geometry& g, int64_t lie_dim, int64_t m, void* scratch,
+                        double* out_logsig, int64_t ld_logsig, int64_t* ld_lie);
 
 // Stream::refine_interval (streams/src/stream.cpp:37-71) for a batch of
 // clopen queries against a support, then to_dyadic_intervals
