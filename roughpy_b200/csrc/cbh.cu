@@ -110,6 +110,13 @@ RPYB_API int rpyb_cbh(int32_t width, int32_t depth, int64_t n_lists, const int64
             std::vector<int64_t> loff(m + 1), rows(nf);
             for (int64_t i = 0; i <= m; ++i) loff[i] = offsets_host[q0 + i] - f0;
             for (int64_t i = 0; i < nf; ++i) rows[i] = i;
+            if (chain && chain_lie_available(g, *maps)) {
+                // products, log and Hall projection in one kernel
+                if ((rc = chain_products_lie(RPYB_F64, g, m, ex, loff, rows, *maps,
+                                             out + q0 * ld_out, ld_out, s)))
+                    return rc;
+                continue;
+            }
             if ((rc = chain ? chain_products(RPYB_F64, g, m, acc, ex, loff, rows, true, s)
                             : ordered_products(RPYB_F64, RPYB_F64, g, m, acc, ex, loff, rows, s)))
                 return rc;

@@ -164,6 +164,19 @@ RPYB_API int rpyb_piecewise_query(int32_t width, int32_t depth, int64_t n_pieces
             std::vector<int64_t> loff(m + 1), rows(nf);
             for (int64_t i = 0; i <= m; ++i) loff[i] = qoff[q0 + i] - f0;
             for (int64_t i = 0; i < nf; ++i) rows[i] = i;
+            if (chain && chain_lie_available(g, *maps)) {
+                // products, log and Hall projection in one kernel
+                double* lsq = out_logsig ? out_logsig + q0 * ld_logsig : nullptr;
+                int64_t ld_lie = 0;
+                double* lie = finish_lie_rows(g, L, m, fin_mem, lsq, ld_logsig, &ld_lie);
+                if ((rc = chain_products_lie(RPYB_F64, g, m, ex, loff, rows, *maps, lie, ld_lie,
+                                             s)) ||
+                    (rc = finish_queries(g, *maps, m, acc, true, lsq, ld_logsig,
+                                         out_sig ? out_sig + q0 * ld_sig : nullptr, ld_sig,
+                                         fin_mem, fin_b, s, true)))
+                    return rc;
+                continue;
+            }
             if ((rc = chain ? chain_products(RPYB_F64, g, m, acc, ex, loff, rows, true, s)
                             : ordered_products(RPYB_F64, RPYB_F64, g, m, acc, ex, loff, rows, s)))
                 return rc;
