@@ -108,6 +108,63 @@ void range_nodes(const rpyb_dyadic_tree* t, int64_t a, int64_t e, std::vector<in
     }
 }
 
+// Leaves of at most one level-1 event: exp(x) written directly, one warp per
+// leaf.  Word (a_1 .. a_k) of exp(x) is x_{a_1} ... x_{a_k} / k!; the words of
+// level depth-1 are formed once and extended by every last letter for the
+// top level.  Computed in float64, rounded once to the tree's type; an empty
+// leaf is the unit.
+struct LeafExpArgs {
+    int32_t width = 0, depth = 0;
+    int64_t T = 0;
+    int64_t db[kMaxDepth + 2] = {};
+    int64_t pw[kMaxDepth + 1] = {};
+    double inv_fact[kMaxDepth + 1] = {};
+};
+
+template <typename T>
+__global__ void leaf_exp_kernel(const LeafExpArgs a, T* __restrict__ nodes,
+                                const T* __restrict__ rows, const int64_t* __restrict__ off,
+                                int64_t n_leaves)
+{
+    __shared__ double xs_all[8][16];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* xs = xs_all[wib];
+    const int d = a.width, N = a.depth;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t leaf = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; leaf < n_leaves;
+         leaf += nwarps) {
+        T* __restrict__ o = nodes + leaf * a.T;
+        const int64_t e0 = off[leaf];
+        __syncwarp();
+        if (off[leaf + 1] == e0) {
+            for (int64_t i = lane; i < a.T; i += 32) o[i] = (i == 0) ? T(1) : T(0);
+            continue;
+        }
+        if (lane < d) xs[lane] = (double)rows[e0 * d + lane];
+        __syncwarp();
+        // levels 0 .. depth-1 word by word
+        for (int k = 0; k <= N - 1; ++k) {
+            const int64_t nk = a.pw[k];
+            for (int64_t w = lane; w < nk; w += 32) {
+                double v = a.inv_fact[k];
+                int64_t r = w;
+                for (int i = 0; i < k; ++i) {
+                    const int64_t q = r / d;
+                    v *= xs[r - q * d];
+                    r = q;
+                }
+                o[a.db[k] + w] = (T)v;
+                if (k == N - 1 && N >= 1) {
+                    // the top level: (w, b) = word w * x_b / N
+                    const double p = v / (double)N;
+                    T* top = o + a.db[N] + w * d;
+                    for (int b = 0; b < d; ++b) top[b] = (T)(p * xs[b]);
+                }
+            }
+        }
+    }
+}
+
 // float64 accumulator rows acc[i] -> tree-typed rows dst[i] (mode's type)
 template <typename T>
 __global__ void store_rows_kernel(T* __restrict__ nodes, int64_t T_, const double* __restrict__ acc,
@@ -118,6 +175,14 @@ __global__ void store_rows_kernel(T* __restrict__ nodes, int64_t T_, const doubl
         const int64_t r = e / T_, c = e - r * T_;
         nodes[dst[r] * T_ + c] = (T)acc[e];
     }
+}
+
+// the most events any leaf holds
+int64_t max_leaf_events(const std::vector<int64_t>& off)
+{
+    int64_t most = 0;
+    for (size_t i = 0; i + 1 < off.size(); ++i) most = std::max(most, off[i + 1] - off[i]);
+    return most;
 }
 
 int build_levels(rpyb_dyadic_tree* t, cudaStream_t s)
@@ -260,6 +325,40 @@ RPYB_API int rpyb_dyadic_build(int mode, int32_t width, int32_t depth, int32_t r
         return fail_release(rc);
     if (n_events == 0) {
         if ((rc = unit_rows(mode, t->nodes, T, T, nullptr, n_leaves, s))) return fail_release(rc);
+    } else if (row_len == width && max_leaf_events(off) <= 1 && width <= 16) {
+        // at most one event per leaf: exp(x) directly
+        LeafExpArgs la;
+        la.width = width;
+        la.depth = depth;
+        la.T = T;
+        for (int k = 0; k <= kMaxDepth + 1; ++k) la.db[k] = g.db[k];
+        double f = 1.0;
+        for (int k = 0; k <= kMaxDepth; ++k) {
+            la.pw[k] = g.pw[k];
+            if (k > 0) f *= (double)k;
+            la.inv_fact[k] = 1.0 / f;
+        }
+        Scratch sc(nullptr, 0, s);
+        void* mem = nullptr;
+        if ((rc = sc.get((size_t)(n_leaves + 1) * 8, &mem))) return fail_release(rc);
+        int64_t* d_off = static_cast<int64_t*>(mem);
+        if (cudaMemcpyAsync(d_off, off.data(), (size_t)(n_leaves + 1) * 8, cudaMemcpyHostToDevice,
+                            s) != cudaSuccess)
+            return fail_release(cuda_fail(cudaGetLastError(), "cudaMemcpyAsync"));
+        const unsigned blocks = (unsigned)std::min<int64_t>((n_leaves + 7) / 8, 148 * 64);
+        if (mode == RPYB_F64)
+            leaf_exp_kernel<double><<<blocks, 256, 0, s>>>(
+                la, static_cast<double*>(t->nodes), static_cast<const double*>(rows), d_off,
+                n_leaves);
+        else
+            leaf_exp_kernel<float><<<blocks, 256, 0, s>>>(
+                la, static_cast<float*>(t->nodes), static_cast<const float*>(rows), d_off,
+                n_leaves);
+        if (cudaGetLastError() != cudaSuccess)
+            return fail_release(fail(RPYB_E_CUDA, "leaf_exp_kernel launch"));
+        // the host offsets must outlive the asynchronous copy
+        if (cudaStreamSynchronize(s) != cudaSuccess)
+            return fail_release(cuda_fail(cudaGetLastError(), "cudaStreamSynchronize"));
     } else if (row_len == width) {
         // Chen products of exp(increment) per leaf, longest leaves first
         std::vector<int64_t> order(n_leaves);
