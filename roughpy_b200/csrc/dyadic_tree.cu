@@ -97,11 +97,21 @@ int64_t node_row(const rpyb_dyadic_tree* t, int64_t level, int64_t blk)
 // and skipped).
 void range_nodes(const rpyb_dyadic_tree* t, int64_t a, int64_t e, std::vector<int64_t>& out)
 {
+    const int64_t l0 = t->lo[0], h0 = t->lo[0] + t->cnt[0];
     while (a < e) {
-        int j = 0;
-        while (j < t->J && (a >> (j + 1)) * ((int64_t)2 << j) == a && a + ((int64_t)2 << j) <= e &&
-               node_row(t, j + 1, a >> (j + 1)) >= 0)
-            ++j;
+        int j;
+        if (a >= l0 && a < h0) {
+            // the tree holds every block containing a leaf of its range: the
+            // block is the largest one aligned at a that fits [a, e)
+            const int tz = a == 0 ? 62 : __builtin_ctzll((unsigned long long)a);
+            const int lg = 63 - __builtin_clzll((unsigned long long)(e - a));
+            j = std::min(std::min(tz, lg), (int)t->J);
+        } else {
+            j = 0;
+            while (j < t->J && (a >> (j + 1)) * ((int64_t)2 << j) == a &&
+                   a + ((int64_t)2 << j) <= e && node_row(t, j + 1, a >> (j + 1)) >= 0)
+                ++j;
+        }
         const int64_t row = node_row(t, j, a >> j);
         if (row >= 0) out.push_back(row);
         a += (int64_t)1 << j;
