@@ -150,6 +150,14 @@ def test_report_error_matches_the_float64_comparison(w, d):
         out2.data_ptr(), plan.size, plan.order.data_ptr(), err2.data_ptr(), ws.data_ptr(),
         nb, torch.cuda.current_stream().cuda_stream))
     torch.cuda.synchronize()
-    assert torch.equal(out2, out) and torch.equal(err2, err)
+    if plan.schedule()["seg"] == 0:
+        # whole streams: the same arithmetic whatever the lane shape
+        assert torch.equal(out2, out) and torch.equal(err2, err)
+    else:
+        # the tuned plan cuts streams into time segments merged by Chen
+        # products: the same values up to float32 rounding
+        o2 = out2.cpu().numpy()
+        assert max(level_rel_err(o2[s:s + 1], o[s:s + 1], w, d) for s in range(len(lens))) <= 2e-6
+        assert float((err2 - err).abs().max()) <= 1e-6
     _, e64 = S.SignaturePlan(off, w, d, "f64").run(x.double(), report_error=True)
     assert float(e64.abs().max()) == 0.0
