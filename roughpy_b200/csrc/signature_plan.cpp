@@ -420,7 +420,7 @@ std::vector<Schedule> candidates(const rpyb_sig_plan* p)
     const int64_t lanes = signature_lanes_per_stream(p->mode, p->width, p->depth, gs[0]);
     const int64_t warp_items = p->n_streams * ((lanes + 31) / 32);
     if (warp_items < (int64_t)sms * 8 * 4) {
-        for (int64_t L : {32, 64, 128, 256, 1024, 4096, 16384})
+        for (int64_t L : {256, 1024, 4096, 16384})
             if (2 * L <= p->max_len) segs.push_back(L);
     }
     for (int i = 0; i < count; ++i)

@@ -92,7 +92,14 @@ def test_host_pipelined_entry_matches_device_path(mode, chunks):
     out_h = torch.full((len(lens), plan.size), float("nan"), dtype=plan.dtype).pin_memory()
     plan.run_host_pipelined(inc_h, out_h, n_chunks=chunks)
     torch.cuda.synchronize()
-    assert torch.equal(out_h, want)
+    if plan.schedule()["seg"] == 0:
+        assert torch.equal(out_h, want)
+    else:
+        # the host entry runs whole streams; a tuned plan may cut them into
+        # time segments: equal up to the mode's rounding
+        tol = 1e-12 if mode == "f64" else 2e-6
+        o, g = out_h.numpy(), want.numpy()
+        assert max(level_rel_err(o[s:s + 1], g[s:s + 1], w, d) for s in range(len(lens))) <= tol
 
 
 @pytest.mark.parametrize("mode", ["f64", "f32c"])
