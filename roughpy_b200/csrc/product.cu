@@ -702,10 +702,17 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
             if (sizeof(T) == 8)
                 product_kernel_blocked<T, TR, 4, 2, ACC, 4><<<grid, kThreads, 0, stream>>>(a);
             else
-                product_kernel_blocked<T, TR, 4, 4, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+                product_kernel_blocked<T, TR, 4, 4, ACC, 4><<<grid, kThreads, 0, stream>>>(a);
             break;
         case 5: product_kernel_blocked<T, TR, 5, 5, ACC, 2><<<grid, kThreads, 0, stream>>>(a); break;
-        case 6: product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a); break;
+        case 6:
+            // float32 rows: four resident blocks (a few spilled registers cost
+            // less than the lost occupancy)
+            if (sizeof(T) == 4)
+                product_kernel_blocked<T, TR, 6, 3, ACC, 4><<<grid, kThreads, 0, stream>>>(a);
+            else
+                product_kernel_blocked<T, TR, 6, 3, ACC, 3><<<grid, kThreads, 0, stream>>>(a);
+            break;
         case 8:
             if (sizeof(T) == 4 && sizeof(TR) == 4 && f32_wide_blocks()) {
                 if (pipe)
