@@ -755,8 +755,9 @@ def profile_queries(nq, log2_events=16):
     """The dyadic-query workload's tree (2^16 events, width 6, depth 5,
     resolution 16, float32 nodes; 2^log2_events events at resolution
     log2_events for a smaller capture) and one query call of nq
-    log-signatures: one fused chain-product-and-log pass and one Hall
-    projection per chunk of 8192 queries."""
+    log-signatures: one fused chain-product, log and Hall-projection launch
+    per chunk of 8192 queries (after the range-product table's launches when
+    nq >= 1024)."""
     import torch
     from roughpy_b200.streams import LieIncrementStream
     n = 1 << log2_events
