@@ -11,7 +11,10 @@
 // (L_k, R_k, old out_k) are coalesced across consecutive units.  The (level,
 // unit) pairs of all output levels are flattened into one index space that
 // is cut into tiles; blockIdx.x walks tiles of one row so that a row's lower
-// levels stay hot in L2, blockIdx.y walks rows.
+// levels stay hot in L2, blockIdx.y walks rows.  Float64 rows of width 2
+// take their levels >= 8 from a kernel whose 32 lanes own the last five
+// letters of a word instead (product_kernel_w2: every load one coalesced
+// request or one broadcast).
 //
 // Arithmetic.  float64: the terms are added in the reference order (lhs
 // degree from high to low, free_tensor_fma.hpp:31-46) with FMA.  float32: by
@@ -218,7 +221,7 @@ product_kernel(const KArgs a)
 // row, word by word, by the threads of the row's first tile: the same terms
 // in the same order as product_kernel, so the blocked kernels need no
 // second launch for them.
-template <typename T, typename TR, typename AccT>
+template <typename T, typename TR, typename AccT, bool POW2 = false>
 __device__ __forceinline__ void small_levels(const KArgs& a, T* __restrict__ out,
                                              const T* __restrict__ lhs,
                                              const TR* __restrict__ rhs,
@@ -243,7 +246,15 @@ __device__ __forceinline__ void small_levels(const KArgs& a, T* __restrict__ out
                 if (p > a.pmax[k]) continue;
                 const int sdeg = k - p;
                 const int64_t ds = a.pw[sdeg];
-                const int64_t li = w / ds, ri = w - li * ds;
+                int64_t li, ri;
+                if constexpr (POW2) {
+                    // width 2: ds = 2^sdeg
+                    li = w >> sdeg;
+                    ri = w & (ds - 1);
+                } else {
+                    li = w / ds;
+                    ri = w - li * ds;
+                }
                 const T lv = (p == 0) ? lhs0 : __ldg(lhs + a.db[p] + li);
                 acc.add(lv, T(__ldg(rhs + a.db[sdeg] + ri)));
             }
@@ -540,6 +551,166 @@ product_kernel_blocked_l(const KArgs a)
     }
 }
 
+// Width-2 kernel for output levels k >= 6 + E (H = 2^E): the 32 lanes of a
+// warp own the last five letters of a word, so that every right-factor run
+// and every streamed top-level word is one coalesced request and every
+// left-factor word one broadcast.  (The blocked kernels above give a thread
+// V consecutive words, and their loads of one word per thread are 32 bytes
+// apart across the warp.)  A thread owns the 2 H words
+//   w(u, i) = u 2^(k-1) + (h0 + i) 32 + lane      (u < 2, i < H)
+// for one block h0 (a multiple of H) of middle parts.  A split point with a
+// right part of s letters (left part p = k - s) reads
+//   s >= 5 + E:      L_p[u 2^(p-1) + (h0 >> (s-5))] (2 broadcasts) and the
+//                    H runs R_s[((h0 mod 2^(s-5)) + i) 32 + lane];
+//   5 <= s < 5 + E:  L_p[u 2^(p-1) + (h0 >> e) + (i >> e)] and
+//                    R_s[(i mod 2^e) 32 + lane], e = s - 5;
+//   s < 5:           R_s[lane mod 2^s] (one word per lane) and the 2 H runs
+//                    L_p[u 2^(p-1) + (h0 + i) 2^(5-s) + (lane >> s)].
+// The terms of a word are added in the same order as in the other kernels
+// (left degree from k down to 0), so the results are the same bits.  Index
+// arithmetic is 32-bit within a row; level k starts at word 2^k - 1.
+template <typename T, typename TR, int H, int ACC = 0, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB)
+product_kernel_w2(const KArgs a)
+{
+    constexpr int E = (H == 1) ? 0 : (H == 2) ? 1 : (H == 4) ? 2 : 3;
+    static_assert((1 << E) == H, "H must be 1, 2, 4 or 8");
+    using AccT = typename AccSel<T, ACC>::type;
+    const int64_t f_begin = (int64_t)blockIdx.x * a.tile_r;
+    const int64_t f_end = min(f_begin + a.tile_r, a.ftotal);
+    const uint32_t lane = threadIdx.x & 31u;
+
+    for (int64_t b = blockIdx.y; b < a.batch; b += gridDim.y) {
+        const int64_t ro = a.out_idx ? a.out_idx[b] : b;
+        const int64_t rl = a.lhs_idx ? a.lhs_idx[b] : b;
+        const int64_t rr = a.rhs_idx ? a.rhs_idx[b] : b;
+        T* __restrict__ out = static_cast<T*>(a.out) + ro * a.ld_out;
+        const T* __restrict__ lhs = static_cast<const T*>(a.lhs) + rl * a.ld_lhs;
+        const TR* __restrict__ rhs = static_cast<const TR*>(a.rhs) + rr * a.ld_rhs;
+        const T* __restrict__ add =
+            a.addend ? static_cast<const T*>(a.addend) + ro * a.ld_add : nullptr;
+        const T lhs0 = (a.lhs0_from_mem ? __ldg(lhs) : T(0)) + T(a.lhs0_add);
+        const T rhs0 = T(__ldg(rhs));
+        if (blockIdx.x == 0) small_levels<T, TR, AccT, true>(a, out, lhs, rhs, add, lhs0);
+
+        // a warp's 32 consecutive units share k and h0 (tiles and level
+        // starts are multiples of 32 units)
+        for (int64_t f = f_begin + threadIdx.x; f < f_end; f += kThreads) {
+            int k = a.klo;
+            while (f >= a.fcum[k + 1]) ++k;
+            const uint32_t rp = (uint32_t)(f - a.fcum[k]);
+            const uint32_t h0 = (rp >> 5) << E;
+            const uint32_t half = 1u << (k - 1);
+            const uint32_t wb = ((1u << k) - 1u) + h0 * 32u + lane;   // word (0, 0) in the row
+            if (a.prefetch && a.pmin[k] <= 0 && a.pmax[k] >= 0) {
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+#pragma unroll
+                    for (int i = 0; i < H; ++i) prefetch_l2(rhs + wb + u * half + 32u * i);
+            }
+
+            AccT acc[2][H];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int i = 0; i < H; ++i)
+                    acc[u][i].init(a.accumulate ? out[wb + u * half + 32u * i] : T(0));
+
+            const int pmax = a.pmax[k];
+            const int pmin = a.pmin[k];
+            if (pmax >= pmin) {
+                if (k <= pmax && k >= pmin) {
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+#pragma unroll
+                        for (int i = 0; i < H; ++i)
+                            acc[u][i].add(__ldg(lhs + wb + u * half + 32u * i), rhs0);
+                }
+                // right parts of 1..4 letters: one right word per lane
+#pragma unroll
+                for (int s = 1; s <= 4; ++s) {
+                    const int p = k - s;
+                    if (p <= pmax && p >= pmin) {
+                        const T rv = T(__ldg(rhs + ((1u << s) - 1u) + (lane & ((1u << s) - 1u))));
+                        const uint32_t lb = ((1u << p) - 1u) + h0 * (32u >> s) + (lane >> s);
+                        const uint32_t lh = 1u << (p - 1);
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+#pragma unroll
+                            for (int i = 0; i < H; ++i)
+                                acc[u][i].add(__ldg(lhs + lb + u * lh + (32u >> s) * i), rv);
+                    }
+                }
+                // right parts of 5 .. 4 + E letters
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int s = 5 + e;
+                    const int p = k - s;
+                    if (p <= pmax && p >= pmin) {
+                        const int nr = 1 << e;
+                        T rv[H];
+#pragma unroll
+                        for (int c = 0; c < nr; ++c)
+                            rv[c] = T(__ldg(rhs + ((1u << s) - 1u) + 32u * c + lane));
+                        const uint32_t lb = ((1u << p) - 1u) + (h0 >> e);
+                        const uint32_t lh = 1u << (p - 1);
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+#pragma unroll
+                            for (int g = 0; g < (H >> e); ++g) {
+                                const T lv = __ldg(lhs + lb + u * lh + g);
+#pragma unroll
+                                for (int c = 0; c < nr; ++c) acc[u][g * nr + c].add(lv, rv[c]);
+                            }
+                    }
+                }
+                // right parts of 5 + E .. k - 1 letters: H runs, 2 broadcasts
+                for (int s = 5 + E; s <= k - 1; ++s) {
+                    const int p = k - s;
+                    if (p <= pmax && p >= pmin) {
+                        const uint32_t rb =
+                            ((1u << s) - 1u) + (h0 & ((1u << (s - 5)) - 1u)) * 32u + lane;
+                        T rv[H];
+#pragma unroll
+                        for (int i = 0; i < H; ++i) rv[i] = T(__ldg(rhs + rb + 32u * i));
+                        const uint32_t lb = ((1u << p) - 1u) + (h0 >> (s - 5));
+                        const T lv0 = __ldg(lhs + lb);
+                        const T lv1 = __ldg(lhs + lb + (1u << (p - 1)));
+#pragma unroll
+                        for (int i = 0; i < H; ++i) {
+                            acc[0][i].add(lv0, rv[i]);
+                            acc[1][i].add(lv1, rv[i]);
+                        }
+                    }
+                }
+                if (pmin <= 0 && pmax >= 0) {
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+#pragma unroll
+                        for (int i = 0; i < H; ++i)
+                            acc[u][i].add(lhs0, T(__ldg(rhs + wb + u * half + 32u * i)));
+                }
+            }
+
+            const T sc = T(a.scale[k]);
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int i = 0; i < H; ++i) {
+                    const uint32_t o = wb + u * half + 32u * i;
+                    T v;
+                    if (a.accumulate) {
+                        v = acc[u][i].value();
+                    } else {
+                        v = sc * acc[u][i].value();
+                        if (add) v += add[o];
+                    }
+                    out[o] = v;
+                }
+        }
+    }
+}
+
 template <typename TD, typename TS>
 __global__ void convert_rows_kernel(TD* dst, int64_t ld_dst, const TS* src, int64_t ld_src,
                                     int64_t cols, int64_t batch)
@@ -729,26 +900,60 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
     return RPYB_OK;
 }
 
+// Width 2 from level kW2Low up, float64 rows: product_kernel_w2 with H =
+// kW2H middle parts per thread (RPYB_W2_KERNEL=0 keeps the blocked kernel).
+// Measured on B200, config 2 at (2,12), % of HBM: float64 46 -> 61; float32
+// rows 35 -> 33 (their F2F conversions bound them, and this kernel converts
+// every loaded word), so float32 and mixed rows keep the blocked kernel.
+constexpr int kW2H = 4;
+constexpr int kW2Low = 8;   // 6 + log2(kW2H): 2^(k-1) >= 32 kW2H words per first letter
+
+bool w2_kernel_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("RPYB_W2_KERNEL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// five resident blocks (48 registers); four were slower on B200 ((2,12):
+// 53 against 61 % of HBM)
+int dispatch_w2(const KArgs& a, dim3 grid, cudaStream_t stream)
+{
+    product_kernel_w2<double, double, kW2H, 0, 5><<<grid, kThreads, 0, stream>>>(a);
+    RPYB_CUDA(cudaGetLastError());
+    return RPYB_OK;
+}
+
 }  // namespace
 
+enum LaunchMode { kSuffix = 0, kBlocked = 1, kW2 = 2 };
+
 static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
-                         const ProductRows& rows, cudaStream_t stream, bool blocked);
+                         const ProductRows& rows, cudaStream_t stream, int mode);
 
 int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
                    const ProductRows& rows, cudaStream_t stream)
 {
     if (rows.batch <= 0) return RPYB_OK;
+    // float64 rows of width 2 with a level of at least 2^kW2Low words: the
+    // lane-letter kernel
+    if (dtype == RPYB_F64 && blocked_enabled() && g.width == 2 && w2_kernel_enabled() &&
+        spec.khi >= kW2Low)
+        return launch_levels(dtype, g, spec, rows, stream, kW2);
     const int L = blocked_enabled() ? blocked_l(g.width) : 0;
     const int kb = std::max(L + 1, spec.klo);
-    if (L == 0 || spec.khi < kb) return launch_levels(dtype, g, spec, rows, stream, false);
+    if (L == 0 || spec.khi < kb) return launch_levels(dtype, g, spec, rows, stream, kSuffix);
     // one blocked launch: levels kb..khi by units, levels klo..L and the
     // level-0 rule word by word in each row's first tile
-    return launch_levels(dtype, g, spec, rows, stream, true);
+    return launch_levels(dtype, g, spec, rows, stream, kBlocked);
 }
 
 static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
-                         const ProductRows& rows, cudaStream_t stream, bool blocked)
+                         const ProductRows& rows, cudaStream_t stream, int mode)
 {
+    const bool blocked = mode != kSuffix;
     KArgs a{};
     a.width = g.width;
     a.klo = std::max(1, spec.klo);
@@ -756,7 +961,7 @@ static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
     a.sklo = 1;
     a.skhi = 0;
     if (blocked) {
-        const int Lb = blocked_l(g.width);
+        const int Lb = mode == kW2 ? kW2Low - 1 : blocked_l(g.width);
         a.sklo = a.klo;
         a.skhi = std::min(spec.khi, Lb);
         a.klo = std::max(Lb + 1, spec.klo);
@@ -767,11 +972,12 @@ static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
     for (int k = 0; k <= kMaxDepth + 1; ++k) a.fcum[k] = 0;
     // work units per level: suffixes (one per d^(k-1)) or, blocked, one per
     // middle part and last-letter block (d^(k-2) * d / V)
-    const int V = blocked ? blocked_v(g.width, dtype != RPYB_F32) : 0;
-    const int L = blocked ? blocked_l(g.width) : 0;
+    const int V = mode == kW2 ? 2 * kW2H : blocked ? blocked_v(g.width, dtype != RPYB_F32) : 0;
+    const int L = mode == kBlocked ? blocked_l(g.width) : 0;
     for (int k = a.klo; k <= a.khi; ++k) {
         a.fcum[k] = f;
-        if (!blocked) f += g.pw[k - 1];
+        if (mode == kW2) f += g.pw[k - 1] / kW2H;   // a multiple of 32 for k >= kW2Low
+        else if (!blocked) f += g.pw[k - 1];
         else if (L == 1) f += g.pw[k - 2] * (g.width / V);
         else f += g.pw[k - 1 - L];
     }
@@ -807,12 +1013,13 @@ static int launch_levels(int dtype, const Geometry& g, const ProductSpec& spec,
 
     // Work units per tile: about kTileWords output words per CTA (at least
     // one unit per thread).
-    const int64_t words_per_unit = blocked ? (int64_t)g.width * V : g.width;
+    const int64_t words_per_unit = mode == kW2 ? V : blocked ? (int64_t)g.width * V : g.width;
     a.tile_r = std::max<int64_t>(kThreads, tile_words() / std::max<int64_t>(1, words_per_unit));
     int64_t tiles = (a.ftotal + a.tile_r - 1) / a.tile_r;
     if (tiles == 0) tiles = 1;  // level 0 only
     if (tiles > 0x7fffffff) return fail(RPYB_E_UNSUPPORTED, "tensor too large");
     dim3 grid((unsigned)tiles, (unsigned)std::min<int64_t>(rows.batch, 65535), 1);
+    if (mode == kW2) return dispatch_w2(a, grid, stream);   // float64 rows only
     if (blocked) {
         if (dtype == RPYB_F64) return dispatch_blocked<double, double, 0>(a, grid, stream);
         if (dtype == kMixedF64F32) return dispatch_blocked<double, float, 0>(a, grid, stream);
