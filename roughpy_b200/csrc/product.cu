@@ -907,6 +907,11 @@ int dispatch_blocked(const KArgs& a, dim3 grid, cudaStream_t stream)
 // every loaded word), so float32 and mixed rows keep the blocked kernel.
 constexpr int kW2H = 4;
 constexpr int kW2Low = 8;   // 6 + log2(kW2H): 2^(k-1) >= 32 kW2H words per first letter
+// products whose top level is at least this take the kernel.  Below it the
+// levels under kW2Low, computed word by word in one tile per row, weigh too
+// much: config-2 sweep on B200, float64 % of HBM, lane-letter / blocked:
+// depth 12 61 / 46, 11 50 / 43, 10 37 / 35, 9 22 / 24, 8 11 / 13
+constexpr int kW2MinTop = 10;
 
 bool w2_kernel_enabled()
 {
@@ -937,10 +942,10 @@ int launch_product(int dtype, const Geometry& g, const ProductSpec& spec,
                    const ProductRows& rows, cudaStream_t stream)
 {
     if (rows.batch <= 0) return RPYB_OK;
-    // float64 rows of width 2 with a level of at least 2^kW2Low words: the
+    // float64 rows of width 2 up to level kW2MinTop or higher: the
     // lane-letter kernel
     if (dtype == RPYB_F64 && blocked_enabled() && g.width == 2 && w2_kernel_enabled() &&
-        spec.khi >= kW2Low)
+        spec.khi >= kW2MinTop)
         return launch_levels(dtype, g, spec, rows, stream, kW2);
     const int L = blocked_enabled() ? blocked_l(g.width) : 0;
     const int kb = std::max(L + 1, spec.klo);

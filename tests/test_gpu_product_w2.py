@@ -1,5 +1,5 @@
 """The width-2 product kernel for float64 rows (lanes owning the last five
-letters, levels >= 8) gives the same bits as the blocked width-2 kernel it
+letters, levels >= 8 of products reaching level 10) gives the same bits as the blocked width-2 kernel it
 replaces there (RPYB_W2_KERNEL=0, read once per process, so the blocked
 results come from a child process), for products, FMAs and the Horner series
 built on them; float32 rows keep the blocked kernel, and the same comparison
@@ -14,7 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SHAPES = [(2, 8, 3), (2, 9, 5), (2, 12, 3)]
+SHAPES = [(2, 9, 3), (2, 10, 5), (2, 12, 3)]   # depth 9: below the kernel's cutoff
 
 
 def compute_all():
